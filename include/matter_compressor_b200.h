@@ -1,0 +1,163 @@
+/*
+ * matter_compressor_b200.h -- C ABI of the B200 (sm_100a) implementation of
+ * matter-compressor's 16^3 block codec and its archive read/append paths.
+ *
+ * Part 1 re-declares, with identical names, signatures and semantics, the
+ * entry points of the reference's public header that this library replaces;
+ * each cites the reference declaration (src/matter_compressor.h:<line>). A
+ * program built against the reference links against libmc_b200.so unchanged
+ * for these calls. Decoding and encoding run on the GPU; there is no CPU
+ * fallback: without a usable sm_100 device the calls report an error through
+ * mc_b200_last_error() (decode calls also zero their output, append calls
+ * return -1).
+ *
+ * Part 2 adds what the reference has no counterpart for: device-resident
+ * (HBM) archives, batched decodes into device buffers, graph-captured decode
+ * plans and batched encode. Pointers documented as "device" are CUDA device
+ * addresses; `stream` is a cudaStream_t passed as void* (NULL: the library's
+ * per-thread stream, synchronised before return).
+ */
+#ifndef MATTER_COMPRESSOR_B200_H
+#define MATTER_COMPRESSOR_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef uint8_t mc_u8;
+
+/* ======================================================== part 1: drop-in */
+
+/* ---- codec context and presets ---- */
+typedef struct mc_codec_ctx mc_codec_ctx;
+mc_codec_ctx *mc_codec_ctx_new(void);                            /* src/matter_compressor.h:42 */
+void  mc_codec_ctx_free(mc_codec_ctx *ctx);                      /* :43 */
+void  mc_codec_ctx_set_quality(mc_codec_ctx *ctx, float quality);/* :44 */
+float mc_codec_ctx_get_quality(mc_codec_ctx *ctx);               /* :45 */
+void  mc_codec_ctx_set_max_error(mc_codec_ctx *ctx, int tau);    /* :58 */
+int   mc_codec_ctx_get_max_error(mc_codec_ctx *ctx);             /* :59 */
+
+typedef enum {
+    MC_PRESET_ARCHIVAL = 0, MC_PRESET_MASTER = 1, MC_PRESET_HIGH = 2, MC_PRESET_BALANCED = 3,
+    MC_PRESET_STREAMING = 4, MC_PRESET_FAST = 5, MC_PRESET_ULTRAFAST = 6, MC_PRESET_PREVIEW = 7,
+    MC_PRESET_COUNT = 8
+} mc_preset;                                                      /* :74-84 */
+float       mc_apply_preset(mc_codec_ctx *ctx, mc_preset level); /* :88 */
+float       mc_preset_quality(mc_preset level);                  /* :89 */
+int         mc_preset_tau(mc_preset level);                      /* :90 */
+const char *mc_preset_name(mc_preset level);                     /* :91 */
+void  mc_codec_init(void);                                        /* :92 */
+void  mc_codec_set_priors(const uint16_t *plo, const uint16_t *phi); /* :96 */
+
+typedef struct { mc_u8 *p; size_t len, cap; } mc_buf;            /* :99 */
+void  mc_buf_put(mc_buf *b, const void *s, size_t n);             /* :100 */
+
+/* ---- block codec (GPU) ---- */
+int   mc_enc_block(mc_codec_ctx *ctx, const mc_u8 *vox, mc_buf *out, uint32_t *len_out); /* :111 */
+void  mc_dec_block(mc_codec_ctx *ctx, const mc_u8 *payload, uint32_t plen, mc_u8 *dst); /* :114 */
+uint32_t mc_enc_fracmap(const mc_u8 *frac, mc_u8 *out, size_t cap);                    /* :117 */
+void     mc_dec_fracmap(const mc_u8 *in, uint32_t len, mc_u8 *frac);                   /* :118 */
+
+/* ---- archive ---- */
+typedef struct mc_archive mc_archive;
+typedef enum { MC_ABSENT = 0, MC_PRESENT = 1, MC_ZERO = 2 } mc_cover;                   /* :173 */
+#define MC_BLOCKCODEC_CABAC 0u
+mc_archive *mc_archive_open(const char *path, int dim, float quality);                  /* :177 */
+mc_archive *mc_archive_open_dims(const char *path, int nx, int ny, int nz, float quality); /* :180 */
+int      mc_archive_set_block_codec(mc_archive *a, uint32_t codec);                     /* :188 */
+uint32_t mc_archive_block_codec(const mc_archive *a);                                  /* :189 */
+int mc_archive_block_blob(mc_archive *a, uint64_t chunk_off, int bz, int by, int bx,
+                          const uint8_t **ptr, uint32_t *len);                         /* :194 */
+int mc_archive_append_chunk_raw(mc_archive *a, int lod, int cz, int cy, int cx,
+                                const mc_u8 vox[256 * 256 * 256]);                     /* :201 */
+int mc_archive_append_chunk_raw_q(mc_archive *a, int lod, int cz, int cy, int cx,
+                                  const mc_u8 vox[256 * 256 * 256], float q);          /* :206 */
+int mc_archive_append_chunk_ctx(mc_archive *a, mc_codec_ctx *C, int lod, int cz, int cy, int cx,
+                                const mc_u8 vox[256 * 256 * 256]);                     /* :212 */
+int mc_archive_append_chunk_compressed(mc_archive *a, int lod, int cz, int cy, int cx,
+                                       const uint8_t *blob, size_t len);               /* :227 */
+int mc_archive_reserve_index(mc_archive *a, int lod, int cz, int cy, int cx);          /* :235 */
+mc_cover mc_archive_chunk_coverage(mc_archive *a, int lod, int cz, int cy, int cx);    /* :238 */
+uint64_t mc_archive_data_len(mc_archive *a);                                           /* :243 */
+int mc_archive_set_metadata(mc_archive *a, const void *data, size_t len);              /* :250 */
+const char *mc_archive_metadata(mc_archive *a, size_t *out_len);                       /* :251 */
+uint64_t mc_archive_chunk_offset(mc_archive *a, int lod, int cz, int cy, int cx);      /* :255 */
+void mc_archive_decode_block(mc_archive *a, uint64_t chunk_off, int bz, int by, int bx,
+                             mc_u8 *dst);                                              /* :260 */
+void mc_archive_decode_chunk(mc_archive *a, uint64_t chunk_off, mc_u8 *out, int nthreads); /* :265 */
+int mc_archive_append_chunk_par(mc_archive *a, int lod, int cz, int cy, int cx,
+                                const mc_u8 vox[256 * 256 * 256], float q, int nthreads); /* :269 */
+void mc_archive_read_region(mc_archive *a, int lod, long z0, long y0, long x0,
+                            long dz, long dy, long dx, mc_u8 *out, size_t sz, size_t sy,
+                            int nthreads);                                             /* :279 */
+int mc_archive_block_present(mc_archive *a, int lod, int bz, int by, int bx);          /* :287 */
+float mc_archive_block_fraction(mc_archive *a, int lod, int bz, int by, int bx);       /* :292 */
+typedef struct { long z0, y0, x0; } mc_box;                                            /* :299 */
+int mc_archive_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count,
+                            long dz, long dy, long dx, float min_frac, mc_box *out);  /* :300 */
+void mc_archive_read_regions(mc_archive *a, int lod, const mc_box *boxes, int n,
+                             long dz, long dy, long dx, mc_u8 *out, size_t batch_stride,
+                             int nthreads);                                            /* :307 */
+void mc_archive_close(mc_archive *a);                                                  /* :312 */
+uint64_t mc_chunk_compute_hash(const uint8_t *blob, uint64_t blob_len);                /* :369 */
+long mc_verify_archive(const uint8_t *arc, size_t len, int verbose);                   /* :370 */
+int mc_archive_set_priors(mc_archive *a, const uint16_t plo[8][32], const uint16_t phi[8][32]); /* :377 */
+uint64_t mc_xxh64(const void *data, size_t len, uint64_t seed);            /* src/mc_codec.h:17 */
+
+/* ====================================================== part 2: additions */
+
+/* Runtime. mc_b200_init returns 0 when an sm_100 device is usable, -1 (with
+ * the reason in mc_b200_last_error) otherwise. The last error is per thread. */
+int  mc_b200_init(void);
+const char *mc_b200_last_error(void);
+void mc_b200_clear_error(void);
+/* Blocks of the calling thread's last decode whose corrupt stream was cut
+ * short (Exp-Golomb prefix cap or overflow-pool exhaustion). */
+uint32_t mc_b200_last_bad_blocks(void);
+
+/* Decode n whole chunk blobs held in HOST memory (blob i: blobs[i], blob_lens[i]
+ * bytes, as stored in an archive) into HOST memory, chunk i at
+ * out + i*out_stride (256^3 z,y,x). A NULL blob decodes to zeros. Payload
+ * bytes go host->device, voxels device->host, inside the call. Returns 0. */
+int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *blob_lens, int n,
+                               mc_u8 *out, size_t out_stride);
+
+/* HBM-resident archive: mirror the archive's bytes in device memory (kept in
+ * sync lazily on later calls). Returns 0; dev_base and len (if non-NULL) receive
+ * the device mirror's address and synced length. */
+int mc_b200_archive_sync(mc_archive *a, const uint8_t **dev_base, uint64_t *len);
+
+/* Decode n chunks of the archive (offsets from mc_archive_chunk_offset) into
+ * DEVICE memory, chunk i at d_out + i*out_stride. */
+int mc_b200_decode_chunks_dev(mc_archive *a, const uint64_t *chunk_offs, int n,
+                              mc_u8 *d_out, size_t out_stride, void *stream);
+
+/* mc_archive_read_regions into DEVICE memory: crop i at d_out + i*batch_stride,
+ * dense z,y,x; decode and crop fused. */
+int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
+                             long dz, long dy, long dx, mc_u8 *d_out, size_t batch_stride,
+                             void *stream);
+
+/* Decode plan: the work list, scratch and a CUDA graph of the whole batched
+ * decode of n chunks into DEVICE memory, built once and replayed. */
+typedef struct mc_b200_plan mc_b200_plan;
+mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *chunk_offs, int n,
+                                         mc_u8 *d_out, size_t out_stride);
+int  mc_b200_plan_launch(mc_b200_plan *p, void *stream);
+/* Kernel launches per replay, blocks decoded, and total payload bytes. */
+void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes);
+void mc_b200_plan_free(mc_b200_plan *p);
+
+/* Batched append: encode n chunks (chunk i's 256^3 voxels at HOST vox[i], or
+ * DEVICE memory when vox_on_device) in one batch and install them in order,
+ * byte-identical to n calls of mc_archive_append_chunk_par (C == NULL, q) or
+ * mc_archive_append_chunk_ctx (C != NULL). coords holds n (cz,cy,cx) triples. */
+int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
+                          const mc_u8 *const *vox, int vox_on_device, float q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

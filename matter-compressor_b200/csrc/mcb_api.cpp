@@ -1,0 +1,578 @@
+// mcb_api.cpp -- decode and append entry points of the C ABI.
+//
+// Decode: the host resolves chunks through the index and locates each block's
+// payload (src/mc_archive.c:712-740, src/mc_archive.h:175-206); every block
+// becomes one work item (payload address in the HBM mirror, output address,
+// strides and clip box) and the whole request is decoded by the two kernel
+// stages in one batch. Whole chunks, single blocks, regions and batches of
+// regions are the same operation with different items.
+//
+// Append: chunks are encoded on the device, blobs come back to the host and
+// are installed in call order, so the file is byte-identical to the
+// reference's for the same call sequence (src/mc_archive.c:590-601,861-901).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "mcb_archive.h"
+#include "mcb_tables.h"
+
+using namespace mcb;
+
+namespace {
+
+constexpr size_t kChunkBytes = (size_t)256 * 256 * 256;
+
+inline uint64_t dptr(const void *p) { return (uint64_t)(uintptr_t)p; }
+
+// Items for every block of one present chunk (co > 1) into a 256^3 output.
+void chunk_items(mc_archive *a, uint64_t co, const uint8_t *dbase, int slot, uint8_t *d_chunk_out, DecItem *items) {
+    const ChunkIndex &ix = chunk_index(a->base, co);
+    const uint64_t cur = a->cursor.load(std::memory_order_acquire);
+    for (int bi = 0; bi < kGrid3; ++bi) {
+        const int bz = bi >> 8, by = (bi >> 4) & 15, bx = bi & 15;
+        DecItem &it = items[bi];
+        memset(&it, 0, sizeof it);
+        const uint64_t off = ix.off[bi];
+        if (off && off + ix.len[bi] <= cur) {   // out-of-bounds payload decodes to zeros (src/mc_archive.c:737-738)
+            it.src = dptr(dbase + off);
+            it.len = ix.len[bi];
+        }
+        it.dst = dptr(d_chunk_out + (size_t)(bz * 16) * 65536 + (by * 16) * 256 + bx * 16);
+        it.sz = 65536;
+        it.sy = 256;
+        it.qslot = (uint16_t)slot;
+        it.clip_lo = kClipFullLo;
+        it.clip_hi = kClipFullHi;
+    }
+}
+
+// Items for every zero block of an absent chunk.
+void zero_chunk_items(uint8_t *d_chunk_out, DecItem *items) {
+    for (int bi = 0; bi < kGrid3; ++bi) {
+        const int bz = bi >> 8, by = (bi >> 4) & 15, bx = bi & 15;
+        DecItem &it = items[bi];
+        memset(&it, 0, sizeof it);
+        it.dst = dptr(d_chunk_out + (size_t)(bz * 16) * 65536 + (by * 16) * 256 + bx * 16);
+        it.sz = 65536;
+        it.sy = 256;
+        it.clip_lo = kClipFullLo;
+        it.clip_hi = kClipFullHi;
+    }
+}
+
+// Items for one region of `lod` (src/mc_archive.c:984-1042): every touched
+// block contributes its intersection with the region; voxel (z,y,x) of the
+// region lands at d_origin + z*sz + y*sy + x.
+bool region_items(mc_archive *a, const uint8_t *dbase, int lod, long z0, long y0, long x0, long dz, long dy,
+                  long dx, uint8_t *d_origin, int64_t sz, int64_t sy, std::vector<DecItem> &items) {
+    const long bz0 = z0 >> 4, by0 = y0 >> 4, bx0 = x0 >> 4;
+    const long nbz = ((z0 + dz + 15) >> 4) - bz0, nby = ((y0 + dy + 15) >> 4) - by0,
+               nbx = ((x0 + dx + 15) >> 4) - bx0;
+    const uint64_t cur = a->cursor.load(std::memory_order_acquire);
+    long last_cz = -1, last_cy = -1, last_cx = -1;
+    uint64_t co = 0;
+    int slot = 0;
+    const ChunkIndex *ix = nullptr;
+    for (long w = 0; w < nbz * nby * nbx; ++w) {
+        const long bz = bz0 + w / (nby * nbx), by = by0 + (w / nbx) % nby, bx = bx0 + w % nbx;
+        const long gz = bz * 16, gy = by * 16, gx = bx * 16;
+        const long iz0 = std::max(gz, z0), iz1 = std::min(gz + 16, z0 + dz);
+        const long iy0 = std::max(gy, y0), iy1 = std::min(gy + 16, y0 + dy);
+        const long ix0 = std::max(gx, x0), ix1 = std::min(gx + 16, x0 + dx);
+        if (iz0 >= iz1 || iy0 >= iy1 || ix0 >= ix1) continue;
+        const long cz = bz >> 4, cy = by >> 4, cx = bx >> 4;
+        if (cz != last_cz || cy != last_cy || cx != last_cx) {
+            co = mc_archive_chunk_offset(a, lod, (int)cz, (int)cy, (int)cx);
+            last_cz = cz; last_cy = cy; last_cx = cx;
+            ix = nullptr;
+            if (co > kSlotZero) {
+                slot = qslot(sanitize_q(chunk_q(a, co)));
+                if (slot < 0) return false;
+                ix = &chunk_index(a->base, co);
+            }
+        }
+        DecItem it;
+        memset(&it, 0, sizeof it);
+        if (ix) {
+            // re-fetch: the thread-local index may have been rebuilt for another chunk
+            ix = &chunk_index(a->base, co);
+            const int bi = (int)(((bz & 15) * 16 + (by & 15)) * 16 + (bx & 15));
+            const uint64_t off = ix->off[bi];
+            if (off && off + ix->len[bi] <= cur) {
+                it.src = dptr(dbase + off);
+                it.len = ix->len[bi];
+            }
+        }
+        it.dst = dptr(d_origin + (gz - z0) * sz + (gy - y0) * sy + (gx - x0));
+        it.sz = sz;
+        it.sy = sy;
+        it.qslot = (uint16_t)slot;
+        it.clip_lo = (uint16_t)(((iz0 - gz) << 8) | ((iy0 - gy) << 4) | (ix0 - gx));
+        it.clip_hi = (uint16_t)(((iz1 - 1 - gz) << 8) | ((iy1 - 1 - gy) << 4) | (ix1 - 1 - gx));
+        items.push_back(it);
+    }
+    return true;
+}
+
+bool finish(Lane &L, cudaStream_t s) { return cuda_ok(cudaStreamSynchronize(s ? s : L.stream), "sync"); }
+
+}  // namespace
+
+// ============================================================ plans
+struct mc_b200_plan {
+    mc_archive *a = nullptr;
+    const uint8_t *mirror = nullptr;
+    DecodeBatch batch;
+    LaunchCfg cfg;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+    long blocks = 0;
+    uint64_t payload = 0;
+};
+
+namespace {
+
+std::mutex g_tune_mu;
+std::map<uint32_t, LaunchCfg> g_tuned;   // per quality (bit pattern)
+
+// Pick CTAs/SM for each stage by timing the real batch (entropy alone, then
+// reconstruction alone) over a small candidate set; cached per quality.
+LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
+    uint32_t key;
+    memcpy(&key, &q, 4);
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return it->second;
+    }
+    LaunchCfg best;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto time_cfg = [&](const LaunchCfg &c) {
+        decode_enqueue(B, c, s);   // warm
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 2; ++r) decode_enqueue(B, c, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    float best_ms = 1e30f;
+    const int ent_opts[] = {2, 3, 4, 5};
+    const int rec_opts[] = {3, 5, 7};
+    for (int e : ent_opts) {
+        LaunchCfg c = best;
+        c.ent_ctas_per_sm = e;
+        float ms = time_cfg(c);
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    best_ms = 1e30f;
+    LaunchCfg base = best;
+    for (int r : rec_opts) {
+        LaunchCfg c = base;
+        c.rec_ctas_per_sm = r;
+        float ms = time_cfg(c);
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tuned[key] = best;
+    return best;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ============================================================ runtime
+int mc_b200_init(void) { return runtime() ? 0 : -1; }
+const char *mc_b200_last_error(void) { return last_error(); }
+void mc_b200_clear_error(void) { clear_error(); }
+uint32_t mc_b200_last_bad_blocks(void) {
+    Lane *L = lane();
+    return L ? lane_bad_blocks(*L) : 0;
+}
+
+// ============================================================ archive decode
+void mc_archive_decode_block(mc_archive *a, uint64_t co, int bz, int by, int bx, mc_u8 *dst) {
+    if (!a || co <= kSlotZero || (unsigned)bz > 15 || (unsigned)by > 15 || (unsigned)bx > 15) {
+        memset(dst, 0, kN3);
+        return;
+    }
+    Lane *L = lane();
+    if (!L) { memset(dst, 0, kN3); return; }
+    const int slot = qslot(sanitize_q(chunk_q(a, co)));
+    uint8_t *dbase = slot < 0 ? nullptr : mirror_sync(a, *L);
+    if (!dbase || !L->out.ensure(kN3) || !L->h_stage.ensure(kN3)) { memset(dst, 0, kN3); return; }
+    const ChunkIndex &ix = chunk_index(a->base, co);
+    const int bi = (bz * 16 + by) * 16 + bx;
+    DecItem it;
+    memset(&it, 0, sizeof it);
+    if (ix.off[bi] && ix.off[bi] + ix.len[bi] <= a->cursor.load(std::memory_order_acquire)) {
+        it.src = dptr(dbase + ix.off[bi]);
+        it.len = ix.len[bi];
+    }
+    it.dst = dptr(L->out.p);
+    it.sz = 256;
+    it.sy = 16;
+    it.qslot = (uint16_t)slot;
+    it.clip_lo = kClipFullLo;
+    it.clip_hi = kClipFullHi;
+    if (!decode_items(*L, &it, 1) ||
+        !cuda_ok(cudaMemcpyAsync(L->h_stage.p, L->out.p, kN3, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
+        !finish(*L, nullptr)) {
+        memset(dst, 0, kN3);
+        return;
+    }
+    memcpy(dst, L->h_stage.p, kN3);
+}
+
+void mc_archive_decode_chunk(mc_archive *a, uint64_t co, mc_u8 *out, int nthreads) {
+    (void)nthreads;
+    if (!a || !out) return;
+    if (co <= kSlotZero) { memset(out, 0, kChunkBytes); return; }
+    Lane *L = lane();
+    if (!L) { memset(out, 0, kChunkBytes); return; }
+    const int slot = qslot(sanitize_q(chunk_q(a, co)));
+    uint8_t *dbase = slot < 0 ? nullptr : mirror_sync(a, *L);
+    if (!dbase || !L->out.ensure(kChunkBytes)) { memset(out, 0, kChunkBytes); return; }
+    std::vector<DecItem> items(kGrid3);
+    chunk_items(a, co, dbase, slot, L->out.as<uint8_t>(), items.data());
+    if (!decode_items(*L, items.data(), kGrid3) ||
+        !cuda_ok(cudaMemcpyAsync(out, L->out.p, kChunkBytes, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
+        !finish(*L, nullptr))
+        memset(out, 0, kChunkBytes);
+}
+
+void mc_archive_read_region(mc_archive *a, int lod, long z0, long y0, long x0, long dz, long dy, long dx,
+                            mc_u8 *out, size_t sz, size_t sy, int nthreads) {
+    (void)nthreads;
+    if (!a || lod < 0 || lod > 7 || !out || dz <= 0 || dy <= 0 || dx <= 0) return;
+    Lane *L = lane();
+    if (!L) return;
+    uint8_t *dbase = mirror_sync(a, *L);
+    const size_t dense = (size_t)dz * dy * dx;
+    if (!dbase || !L->out.ensure(dense)) return;
+    std::vector<DecItem> items;
+    if (!region_items(a, dbase, lod, z0, y0, x0, dz, dy, dx, L->out.as<uint8_t>(), (int64_t)dy * dx, dx, items))
+        return;
+    if (!decode_items(*L, items.data(), (int)items.size())) return;
+    bool ok = true;
+    if (sy == (size_t)dx && sz == (size_t)dy * dx) {
+        ok = cuda_ok(cudaMemcpyAsync(out, L->out.p, dense, cudaMemcpyDeviceToHost, L->stream), "D2H");
+    } else {
+        for (long z = 0; z < dz && ok; ++z)
+            ok = cuda_ok(cudaMemcpy2DAsync(out + z * sz, sy, L->out.as<uint8_t>() + (size_t)z * dy * dx, dx, dx, dy,
+                                           cudaMemcpyDeviceToHost, L->stream),
+                         "D2H");
+    }
+    if (ok) finish(*L, nullptr);
+}
+
+void mc_archive_read_regions(mc_archive *a, int lod, const mc_box *boxes, int n, long dz, long dy, long dx,
+                             mc_u8 *out, size_t batch_stride, int nthreads) {
+    (void)nthreads;
+    if (!a || !boxes || n <= 0 || !out) return;
+    if (lod < 0 || lod > 7 || dz <= 0 || dy <= 0 || dx <= 0) return;   // each crop's read_region returns
+    Lane *L = lane();
+    if (!L) return;
+    uint8_t *dbase = mirror_sync(a, *L);
+    const size_t crop = (size_t)dz * dy * dx;
+    if (!dbase || !L->out.ensure(crop * n)) return;
+    std::vector<DecItem> items;
+    for (int i = 0; i < n; ++i)
+        if (!region_items(a, dbase, lod, boxes[i].z0, boxes[i].y0, boxes[i].x0, dz, dy, dx,
+                          L->out.as<uint8_t>() + crop * i, (int64_t)dy * dx, dx, items))
+            return;
+    if (!decode_items(*L, items.data(), (int)items.size())) return;
+    bool ok = true;
+    if (batch_stride == crop) {
+        ok = cuda_ok(cudaMemcpyAsync(out, L->out.p, crop * n, cudaMemcpyDeviceToHost, L->stream), "D2H");
+    } else {
+        for (int i = 0; i < n && ok; ++i)
+            ok = cuda_ok(cudaMemcpyAsync(out + (size_t)i * batch_stride, L->out.as<uint8_t>() + crop * i, crop,
+                                         cudaMemcpyDeviceToHost, L->stream),
+                         "D2H");
+    }
+    if (ok) finish(*L, nullptr);
+}
+
+// ============================================================ device-output decode
+int mc_b200_archive_sync(mc_archive *a, const uint8_t **dev_base, uint64_t *len) {
+    if (!a) return -1;
+    Lane *L = lane();
+    if (!L) return -1;
+    uint8_t *d = mirror_sync(a, *L);
+    if (!d || !finish(*L, nullptr)) return -1;
+    if (dev_base) *dev_base = d;
+    if (len) *len = a->synced;
+    return 0;
+}
+
+int mc_b200_decode_chunks_dev(mc_archive *a, const uint64_t *offs, int n, mc_u8 *d_out, size_t stride, void *stream) {
+    if (!a || !offs || n < 0 || !d_out) return -1;
+    Lane *L = lane();
+    if (!L) return -1;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+    uint8_t *dbase = mirror_sync(a, *L);
+    if (!dbase) return -1;
+    if (s != L->stream && !cuda_ok(cudaStreamWaitEvent(s, a->mir_ev, 0), "stream wait")) return -1;
+    std::vector<DecItem> items((size_t)n * kGrid3);
+    for (int c = 0; c < n; ++c) {
+        uint8_t *dst = d_out + (size_t)c * stride;
+        if (offs[c] <= kSlotZero) { zero_chunk_items(dst, &items[(size_t)c * kGrid3]); continue; }
+        int slot = qslot(sanitize_q(chunk_q(a, offs[c])));
+        if (slot < 0) return -1;
+        chunk_items(a, offs[c], dbase, slot, dst, &items[(size_t)c * kGrid3]);
+    }
+    if (!decode_items(*L, items.data(), (int)items.size(), s)) return -1;
+    if (!stream && !finish(*L, nullptr)) return -1;
+    return 0;
+}
+
+int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n, long dz, long dy, long dx,
+                             mc_u8 *d_out, size_t batch_stride, void *stream) {
+    if (!a || !boxes || n <= 0 || !d_out || lod < 0 || lod > 7 || dz <= 0 || dy <= 0 || dx <= 0) return -1;
+    Lane *L = lane();
+    if (!L) return -1;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+    uint8_t *dbase = mirror_sync(a, *L);
+    if (!dbase) return -1;
+    if (s != L->stream && !cuda_ok(cudaStreamWaitEvent(s, a->mir_ev, 0), "stream wait")) return -1;
+    std::vector<DecItem> items;
+    for (int i = 0; i < n; ++i)
+        if (!region_items(a, dbase, lod, boxes[i].z0, boxes[i].y0, boxes[i].x0, dz, dy, dx,
+                          d_out + (size_t)i * batch_stride, (int64_t)dy * dx, dx, items))
+            return -1;
+    if (!decode_items(*L, items.data(), (int)items.size(), s)) return -1;
+    if (!stream && !finish(*L, nullptr)) return -1;
+    return 0;
+}
+
+// Blobs in host memory -> voxels in host memory, in groups of chunks.
+int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens, int n, mc_u8 *out,
+                               size_t out_stride) {
+    if (n < 0 || (n && (!blobs || !lens || !out))) return -1;
+    Lane *L = lane();
+    if (!L) return -1;
+    const int G = 16;
+    std::vector<DecItem> items;
+    for (int c0 = 0; c0 < n; c0 += G) {
+        const int g = std::min(G, n - c0);
+        uint64_t total = 0;
+        std::vector<uint64_t> at(g);
+        for (int j = 0; j < g; ++j) {
+            at[j] = total;
+            total += blobs[c0 + j] ? ((lens[c0 + j] + 15) & ~15ull) : 0;
+        }
+        if (!L->src.ensure(total + 64) || !L->out.ensure(kChunkBytes * g)) return -1;
+        items.assign((size_t)g * kGrid3, DecItem{});
+        for (int j = 0; j < g; ++j) {
+            const uint8_t *b = blobs[c0 + j];
+            const uint64_t bl = lens[c0 + j];
+            uint8_t *dchunk = L->out.as<uint8_t>() + kChunkBytes * j;
+            DecItem *it = &items[(size_t)j * kGrid3];
+            zero_chunk_items(dchunk, it);
+            if (!b || bl < (uint64_t)kBlobHdr) continue;
+            if (!cuda_ok(cudaMemcpyAsync(L->src.as<uint8_t>() + at[j], b, bl, cudaMemcpyHostToDevice, L->stream),
+                         "H2D blob"))
+                return -1;
+            // locate payloads (src/mc_archive.h:175-206), bounded by the blob
+            uint16_t fml;
+            memcpy(&fml, b + 12, 2);
+            const uint64_t bm_off = kBlobHdr + (uint64_t)fml;
+            if (bm_off + kBitmapBytes > bl) continue;
+            const uint8_t *bm = b + bm_off;
+            uint32_t np = 0;
+            for (int i = 0; i < kBitmapBytes; ++i) np += (uint32_t)__builtin_popcount(bm[i]);
+            const uint8_t *l16 = bm + kBitmapBytes;
+            if (bm_off + kBitmapBytes + 2ull * np > bl) continue;
+            float q;
+            memcpy(&q, b, 4);
+            const int slot = qslot(sanitize_q(q));
+            if (slot < 0) return -1;
+            uint64_t pay = bm_off + kBitmapBytes + 2ull * np;
+            uint32_t k = 0;
+            for (int bi = 0; bi < kGrid3; ++bi) {
+                it[bi].qslot = (uint16_t)slot;
+                if (!((bm[bi >> 3] >> (bi & 7)) & 1)) continue;
+                uint16_t l;
+                memcpy(&l, l16 + 2 * k, 2);
+                ++k;
+                if (pay + l <= bl) {
+                    it[bi].src = dptr(L->src.as<uint8_t>() + at[j] + pay);
+                    it[bi].len = l;
+                }
+                pay += l;
+            }
+        }
+        if (!decode_items(*L, items.data(), (int)items.size())) return -1;
+        bool ok = true;
+        if (out_stride == kChunkBytes) {
+            ok = cuda_ok(cudaMemcpyAsync(out + kChunkBytes * c0, L->out.p, kChunkBytes * g, cudaMemcpyDeviceToHost,
+                                         L->stream), "D2H");
+        } else {
+            for (int j = 0; j < g && ok; ++j)
+                ok = cuda_ok(cudaMemcpyAsync(out + out_stride * (c0 + j), L->out.as<uint8_t>() + kChunkBytes * j,
+                                             kChunkBytes, cudaMemcpyDeviceToHost, L->stream), "D2H");
+        }
+        if (!ok || !finish(*L, nullptr)) return -1;
+    }
+    return 0;
+}
+
+// ============================================================ plans
+mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *offs, int n, mc_u8 *d_out, size_t stride) {
+    if (!a || !offs || n <= 0 || !d_out) return nullptr;
+    Lane *L = lane();
+    if (!L) return nullptr;
+    uint8_t *dbase = mirror_sync(a, *L);
+    if (!dbase || !finish(*L, nullptr)) return nullptr;
+    mc_b200_plan *p = new mc_b200_plan();
+    p->a = a;
+    p->mirror = dbase;
+    std::vector<DecItem> items((size_t)n * kGrid3);
+    float q_major = 6.0f;
+    for (int c = 0; c < n; ++c) {
+        uint8_t *dst = d_out + (size_t)c * stride;
+        if (offs[c] <= kSlotZero) { zero_chunk_items(dst, &items[(size_t)c * kGrid3]); continue; }
+        float q = sanitize_q(chunk_q(a, offs[c]));
+        q_major = q;
+        int slot = qslot(q);
+        if (slot < 0) { delete p; return nullptr; }
+        chunk_items(a, offs[c], dbase, slot, dst, &items[(size_t)c * kGrid3]);
+    }
+    for (auto &it : items) {
+        p->blocks++;
+        p->payload += it.len;
+    }
+    if (!decode_prepare(p->batch, items.data(), (int)items.size(), L->stream)) { delete p; return nullptr; }
+    p->cfg = autotune(p->batch, q_major, L->stream);
+    cudaStream_t cs = nullptr;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream") &&
+              cuda_ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture") &&
+              decode_enqueue(p->batch, p->cfg, cs);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    ok = ok && cuda_ok(ce, "end capture") && cuda_ok(cudaGraphInstantiate(&p->exec, g, 0), "instantiate");
+    if (cs) cudaStreamDestroy(cs);
+    p->graph = g;
+    if (!ok) { mc_b200_plan_free(p); return nullptr; }
+    p->launches = 2 * (int)p->batch.subs.size();
+    return p;
+}
+
+int mc_b200_plan_launch(mc_b200_plan *p, void *stream) {
+    if (!p || !p->exec) return -1;
+    if (p->a->d_base != p->mirror) {
+        set_error("decode plan is stale: the archive's device mirror moved since the plan was built");
+        return -1;
+    }
+    return cuda_ok(cudaGraphLaunch(p->exec, static_cast<cudaStream_t>(stream)), "graph launch") ? 0 : -1;
+}
+
+void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes) {
+    if (launches) *launches = p ? p->launches : 0;
+    if (blocks) *blocks = p ? p->blocks : 0;
+    if (payload_bytes) *payload_bytes = p ? p->payload : 0;
+}
+
+void mc_b200_plan_free(mc_b200_plan *p) {
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    delete p;
+}
+
+// ============================================================ append
+int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
+                          const mc_u8 *const *vox, int vox_on_device, float q) {
+    if (!a || lod < 0 || lod > 7 || n < 0 || (n && (!coords || !vox))) return -1;
+    for (int i = 0; i < n; ++i)
+        if (!vox[i]) return -1;
+    Lane *L = lane();
+    if (!L) return -1;
+    const int G = 8;
+    std::vector<float> hq(G), qq(G);
+    std::vector<int> tau(G);
+    std::vector<uint64_t> boff, blen;
+    for (int c0 = 0; c0 < n; c0 += G) {
+        const int g = std::min(G, n - c0);
+        std::vector<const uint8_t *> dv(g);
+        if (!vox_on_device && !L->src.ensure(kChunkBytes * g)) return -1;
+        for (int j = 0; j < g; ++j) {
+            if (vox_on_device) {
+                dv[j] = vox[c0 + j];
+            } else {
+                dv[j] = L->src.as<uint8_t>() + kChunkBytes * j;
+                if (!cuda_ok(cudaMemcpyAsync(const_cast<uint8_t *>(dv[j]), vox[c0 + j], kChunkBytes,
+                                             cudaMemcpyHostToDevice, L->stream), "H2D voxels"))
+                    return -1;
+            }
+            if (C) {   // caller's context: its quality and max error (src/mc_archive.c:590-601)
+                hq[j] = qq[j] = C->quality;
+                tau[j] = C->max_err;
+            } else {   // parallel path: raw q in the header, no max error (src/mc_archive.c:864-866)
+                float qv = q > 0 ? q : a->quality;
+                hq[j] = qv;
+                qq[j] = sanitize_q(qv);
+                tau[j] = 0;
+            }
+        }
+        if (!encode_chunks(*L, dv.data(), g, hq.data(), qq.data(), tau.data(), boff, blen)) return -1;
+        uint64_t total = 0;
+        for (int j = 0; j < g; ++j) total = std::max(total, boff[j] + blen[j]);
+        if (!L->h_stage.ensure(total + 16)) return -1;
+        if (total && !cuda_ok(cudaMemcpy(L->h_stage.p, L->blobs.p, total, cudaMemcpyDeviceToHost), "D2H blobs"))
+            return -1;
+        for (int j = 0; j < g; ++j) {
+            const int *cc = coords + 3 * (c0 + j);
+            int rc;
+            if (blen[j]) rc = install_blob(a, lod, cc[0], cc[1], cc[2], L->h_stage.as<uint8_t>() + boff[j], blen[j]);
+            else rc = C ? mark_zero(a, lod, cc[0], cc[1], cc[2]) : 0;   // all air
+            if (rc) return rc;
+        }
+    }
+    return 0;
+}
+
+int mc_archive_append_chunk_par(mc_archive *a, int lod, int cz, int cy, int cx, const mc_u8 vox[256 * 256 * 256],
+                                float q, int nthreads) {
+    (void)nthreads;
+    if (!a || lod < 0 || lod > 7 || !vox) return -1;
+    const int cc[3] = {cz, cy, cx};
+    const mc_u8 *v = vox;
+    return mc_b200_append_chunks(a, nullptr, lod, cc, 1, &v, 0, q);
+}
+
+int mc_archive_append_chunk_ctx(mc_archive *a, mc_codec_ctx *C, int lod, int cz, int cy, int cx,
+                                const mc_u8 vox[256 * 256 * 256]) {
+    if (!a || !C || lod < 0 || lod > 7 || !vox) return -1;
+    const int cc[3] = {cz, cy, cx};
+    const mc_u8 *v = vox;
+    return mc_b200_append_chunks(a, C, lod, cc, 1, &v, 0, 0.0f);
+}
+
+int mc_archive_append_chunk_raw_q(mc_archive *a, int lod, int cz, int cy, int cx, const mc_u8 vox[256 * 256 * 256],
+                                  float q) {
+    if (!a || lod < 0 || lod > 7 || !vox) return -1;
+    mc_codec_ctx C;
+    mc_codec_ctx_set_quality(&C, q);   // throwaway ctx: quality only (src/mc_archive.c:602-611)
+    return mc_archive_append_chunk_ctx(a, &C, lod, cz, cy, cx, vox);
+}
+
+int mc_archive_append_chunk_raw(mc_archive *a, int lod, int cz, int cy, int cx, const mc_u8 vox[256 * 256 * 256]) {
+    return mc_archive_append_chunk_raw_q(a, lod, cz, cy, cx, vox, a ? a->quality : 8.0f);
+}
+
+}  // extern "C"

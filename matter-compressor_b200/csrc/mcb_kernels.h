@@ -1,0 +1,92 @@
+// mcb_kernels.h -- launch interface of the sm_100a kernels (host side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mcb_format.h"
+
+namespace mcb {
+
+// Launch shape knobs, picked per quality by the autotuner.
+struct LaunchCfg {
+    int ent_ctas_per_sm = 8;   // entropy stage: CTAs of 4 warps per SM
+    int rec_ctas_per_sm = 6;   // reconstruction stage: CTAs of 128 threads per SM
+};
+
+struct EntParams {
+    const DecItem *items;
+    const uint32_t *order;     // optional processing order (by payload size), or null
+    int n;
+    const uint64_t *base;      // per-item arena offset (entries)
+    uint32_t *arena;
+    EntHdr *hdr;
+    uint32_t *pool;            // overflow pool for corrupt streams
+    uint32_t pool_cap;
+    uint32_t *pool_used;
+    const QTab *qtab;
+    const uint16_t *scan;      // scan position -> raster idx | band<<12
+    uint32_t *status;          // [0]: blocks whose stream was cut short
+};
+
+struct RecParams {
+    const DecItem *items;
+    int n;
+    const EntHdr *hdr;
+    const uint64_t *base;
+    const uint32_t *arena;
+    const uint32_t *pool;
+    const QTab *qtab;
+};
+
+cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
+cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s);
+cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStream_t s);
+
+// ---- encode ----
+// One 16^3 block to encode, gathered from a strided u8 source.
+struct EncItem {
+    uint64_t src;      // device address of source voxel (0,0,0) of the block
+    int64_t sz, sy;    // source byte strides
+    uint64_t out;      // device address of this block's payload slot (kEncCap bytes)
+    uint16_t qslot;
+    uint16_t tau;      // max-error bound, 0 = off
+    uint32_t pad;
+};
+static_assert(sizeof(EncItem) == 40, "EncItem layout");
+
+struct EncParams {
+    const EncItem *items;
+    int n;
+    const QTab *qtab;
+    const uint16_t *scan;
+    uint32_t *len;       // per item: payload bytes (0 = all air, not coded)
+    uint8_t *frac;       // per item: material nibble
+    uint32_t *status;    // [0]: payloads that overflowed kEncCap
+};
+cudaError_t upload_cos_encode(const float cmf[16][16], cudaStream_t s);
+cudaError_t launch_encode(const EncParams &p, cudaStream_t s);
+
+// Chunk-blob assembly for chunks whose blocks were encoded by launch_encode
+// with items in block order (chunk c owns items [4096c, 4096c+4096)).
+struct BlobParams {
+    int nchunks;
+    const uint8_t *payload;   // item i's payload at payload + i*kEncCap
+    const uint32_t *len;      // per item
+    const uint8_t *frac;      // per item
+    const float *header_q;    // per chunk: q written into the blob header
+    // sizing-pass outputs (side buffers)
+    uint32_t *scratch;        // per item: payload offset within the chunk's payloads
+    uint16_t *lens16;         // per chunk: 4096 u16 length table
+    uint8_t *bitmap;          // per chunk: 512 B
+    uint8_t *fmap;            // per chunk: kFmapCap bytes
+    uint32_t *fml, *np;       // per chunk
+    uint64_t *blob_len;       // per chunk: total blob bytes, 0 = all air
+    // write-pass inputs
+    const uint64_t *blob_off; // per chunk: offset of the blob in `blobs`
+    uint8_t *blobs;
+};
+cudaError_t launch_blob_layout(const BlobParams &p, cudaStream_t s);   // sizing pass
+cudaError_t launch_blob_fill(const BlobParams &p, cudaStream_t s);     // write pass
+cudaError_t launch_blob_hash(const BlobParams &p, cudaStream_t s);     // xxh64 chain
+
+}  // namespace mcb

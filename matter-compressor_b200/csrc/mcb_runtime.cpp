@@ -1,0 +1,324 @@
+// mcb_runtime.cpp -- device runtime (see mcb_runtime.h).
+#include "mcb_runtime.h"
+
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "mcb_tables.h"
+
+namespace mcb {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_err;
+
+bool set_error(const std::string &msg) {
+    t_err = msg;
+    fprintf(stderr, "matter-compressor-b200: %s\n", msg.c_str());
+    return false;
+}
+bool cuda_ok(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return true;
+    return set_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+const char *last_error() { return t_err.empty() ? nullptr : t_err.c_str(); }
+void clear_error() { t_err.clear(); }
+
+// ------------------------------------------------------------------ buffers
+bool DevBuf::ensure(size_t n) {
+    if (n <= cap) return true;
+    size_t want = std::max(n, cap + cap / 2);
+    void *np = nullptr;
+    if (!cuda_ok(cudaMalloc(&np, want), "cudaMalloc")) return false;
+    if (p) {
+        cudaDeviceSynchronize();   // no kernel may still read the old buffer
+        cudaFree(p);
+    }
+    p = np;
+    cap = want;
+    return true;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+bool HostBuf::ensure(size_t n) {
+    if (n <= cap) return true;
+    size_t want = std::max(n, cap + cap / 2);
+    void *np = nullptr;
+    if (!cuda_ok(cudaMallocHost(&np, want), "cudaMallocHost")) return false;
+    if (p) cudaFreeHost(p);
+    p = np;
+    cap = want;
+    return true;
+}
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
+// ------------------------------------------------------------------ runtime
+static Runtime *g_rt = nullptr;
+static std::once_flag g_rt_once;
+static std::string g_rt_err;
+
+static void runtime_init() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        g_rt_err = std::string("no CUDA device available (") + cudaGetErrorString(e) + ")";
+        return;
+    }
+    Runtime *R = new Runtime();
+    cudaGetDevice(&R->device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, R->device) == cudaSuccess) {
+        R->sms = prop.multiProcessorCount;
+        if (prop.major < 10) {
+            g_rt_err = std::string("device ") + prop.name + " is not sm_100 (Blackwell); kernels are built for sm_100a only";
+            delete R;
+            return;
+        }
+    }
+    table_scan(R->h_scan);
+    table_cos(R->h_cos);
+    if (cudaMalloc(&R->d_scan, sizeof R->h_scan) != cudaSuccess ||
+        cudaMalloc(&R->d_qtab, sizeof(QTab) * kMaxQSlots) != cudaSuccess ||
+        cudaMemcpy(R->d_scan, R->h_scan, sizeof R->h_scan, cudaMemcpyHostToDevice) != cudaSuccess ||
+        upload_cos(R->h_cos, 0) != cudaSuccess || upload_cos_encode(R->h_cos, 0) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+        g_rt_err = std::string("device table upload failed: ") + cudaGetErrorString(cudaGetLastError());
+        delete R;
+        return;
+    }
+    g_rt = R;
+}
+
+Runtime *runtime() {
+    std::call_once(g_rt_once, runtime_init);
+    if (!g_rt) set_error(g_rt_err);
+    return g_rt;
+}
+
+int qslot(float q) {
+    Runtime *R = runtime();
+    if (!R) return -1;
+    uint32_t qb;
+    memcpy(&qb, &q, 4);
+    const uint64_t key = ((uint64_t)qb << 32) | priors_generation();
+    std::lock_guard<std::mutex> g(R->qmu);
+    for (size_t i = 0; i < R->qkeys.size(); ++i)
+        if (R->qkeys[i] == key) return (int)i;
+    if (R->qkeys.size() >= (size_t)kMaxQSlots) {
+        // every slot taken: wait for in-flight work, then start over
+        cudaDeviceSynchronize();
+        R->qkeys.clear();
+    }
+    QTab t;
+    table_qtab(q, &t);
+    int slot = (int)R->qkeys.size();
+    if (!cuda_ok(cudaMemcpy(R->d_qtab + slot, &t, sizeof t, cudaMemcpyHostToDevice), "qtab upload")) return -1;
+    R->qkeys.push_back(key);
+    return slot;
+}
+
+// ------------------------------------------------------------------ lanes
+Lane::~Lane() {
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+static thread_local Lane *t_lane = nullptr;
+static thread_local struct LaneOwner { ~LaneOwner() { delete t_lane; t_lane = nullptr; } } t_lane_owner;
+
+Lane *lane() {
+    if (t_lane) return t_lane;
+    if (!runtime()) return nullptr;
+    Lane *L = new Lane();
+    if (!cuda_ok(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking), "stream") ||
+        !cuda_ok(cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming), "event")) {
+        delete L;
+        return nullptr;
+    }
+    (void)t_lane_owner;
+    t_lane = L;
+    return L;
+}
+
+// ------------------------------------------------------------------ decode
+static constexpr uint64_t kArenaMaxEntries = 256ull << 20;   // 1 GiB of entries per sub-batch
+static constexpr uint32_t kPoolEntries = 4u << 20;           // overflow pool, 16 MiB
+
+bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s) {
+    B.n = n;
+    B.subs.clear();
+    if (n <= 0) return true;
+    std::vector<uint64_t> hb((size_t)n);
+    uint64_t max_acc = 1;
+    int i0 = 0;
+    while (i0 < n) {
+        uint64_t acc = 0;
+        int i1 = i0;
+        while (i1 < n) {
+            uint64_t c = entry_cap(h_items[i1].len);
+            if (i1 > i0 && acc + c > kArenaMaxEntries) break;
+            hb[i1] = acc;
+            acc += c;
+            ++i1;
+        }
+        max_acc = std::max(max_acc, acc);
+        B.subs.emplace_back(i0, i1);
+        i0 = i1;
+    }
+    if (!B.items.ensure(sizeof(DecItem) * (size_t)n) || !B.base.ensure(sizeof(uint64_t) * (size_t)n) ||
+        !B.hdr.ensure(sizeof(EntHdr) * (size_t)n) || !B.arena.ensure(sizeof(uint32_t) * max_acc) ||
+        !B.pool.ensure(sizeof(uint32_t) * kPoolEntries) || !B.status.ensure(16))
+        return false;
+    // synchronous copies: the host arrays may be pageable and short-lived
+    return cuda_ok(cudaMemcpyAsync(B.items.p, h_items, sizeof(DecItem) * (size_t)n, cudaMemcpyHostToDevice, s),
+                   "H2D items") &&
+           cuda_ok(cudaMemcpyAsync(B.base.p, hb.data(), sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s),
+                   "H2D base") &&
+           cuda_ok(cudaStreamSynchronize(s), "sync");
+}
+
+bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
+    Runtime *R = runtime();
+    if (!R) return false;
+    if (!cuda_ok(cudaMemsetAsync(B.status.p, 0, 16, s), "memset")) return false;
+    for (auto &r : B.subs) {
+        const int i0 = r.first, m = r.second - r.first;
+        EntParams ep;
+        ep.items = B.items.as<DecItem>() + i0;
+        ep.order = nullptr;
+        ep.n = m;
+        ep.base = B.base.as<uint64_t>() + i0;
+        ep.arena = B.arena.as<uint32_t>();
+        ep.hdr = B.hdr.as<EntHdr>() + i0;
+        ep.pool = B.pool.as<uint32_t>();
+        ep.pool_cap = kPoolEntries;
+        ep.pool_used = B.status.as<uint32_t>() + 1;
+        ep.qtab = R->d_qtab;
+        ep.scan = R->d_scan;
+        ep.status = B.status.as<uint32_t>();
+        if (!cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
+        RecParams rp;
+        rp.items = B.items.as<DecItem>() + i0;
+        rp.n = m;
+        rp.hdr = B.hdr.as<EntHdr>() + i0;
+        rp.base = B.base.as<uint64_t>() + i0;
+        rp.arena = B.arena.as<uint32_t>();
+        rp.pool = B.pool.as<uint32_t>();
+        rp.qtab = R->d_qtab;
+        if (!cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
+    }
+    return true;
+}
+
+bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s) {
+    if (n <= 0) return true;
+    if (!s) s = L.stream;
+    if (!cuda_ok(cudaEventSynchronize(L.done), "event sync")) return false;
+    if (!decode_prepare(L.batch, items, n, s) || !decode_enqueue(L.batch, L.cfg, s)) return false;
+    return cuda_ok(cudaEventRecord(L.done, s), "event record");
+}
+
+uint32_t lane_bad_blocks(Lane &L) {
+    uint32_t v = 0;
+    if (L.batch.status.p) cudaMemcpy(&v, L.batch.status.p, 4, cudaMemcpyDeviceToHost);
+    return v;
+}
+
+// ------------------------------------------------------------------ encode
+bool encode_chunks(Lane &L, const uint8_t *const *d_vox, int nchunks, const float *header_q, const float *q,
+                   const int *tau, std::vector<uint64_t> &blob_off, std::vector<uint64_t> &blob_len) {
+    Runtime *R = runtime();
+    if (!R) return false;
+    blob_off.assign(nchunks, 0);
+    blob_len.assign(nchunks, 0);
+    if (nchunks <= 0) return true;
+    if (!cuda_ok(cudaEventSynchronize(L.done), "event sync")) return false;
+    const size_t n = (size_t)nchunks * kGrid3;
+    if (!L.h_items.ensure(sizeof(EncItem) * n) || !L.enc_items.ensure(sizeof(EncItem) * n) ||
+        !L.enc_len.ensure(4 * n) || !L.enc_frac.ensure(n) || !L.enc_pay.ensure((size_t)kEncCap * n) ||
+        !L.status.ensure(16) || !L.b_scratch.ensure(4 * n) || !L.b_lens16.ensure(2 * n) ||
+        !L.b_bitmap.ensure((size_t)kBitmapBytes * nchunks) || !L.b_fmap.ensure((size_t)kFmapCap * nchunks) ||
+        !L.b_fml.ensure(4 * nchunks) || !L.b_np.ensure(4 * nchunks) || !L.b_len.ensure(8 * nchunks) ||
+        !L.b_off.ensure(8 * nchunks) || !L.b_q.ensure(4 * nchunks) || !L.h_misc.ensure(16 * (size_t)nchunks))
+        return false;
+    EncItem *hi = L.h_items.as<EncItem>();
+    for (int c = 0; c < nchunks; ++c) {
+        int slot = qslot(q[c]);
+        if (slot < 0) return false;
+        for (int bi = 0; bi < kGrid3; ++bi) {
+            int bz = bi >> 8, by = (bi >> 4) & 15, bx = bi & 15;
+            EncItem &it = hi[(size_t)c * kGrid3 + bi];
+            it.src = (uint64_t)(uintptr_t)(d_vox[c] + (size_t)(bz * 16) * 65536 + (by * 16) * 256 + bx * 16);
+            it.sz = 65536;
+            it.sy = 256;
+            it.out = (uint64_t)(uintptr_t)(L.enc_pay.as<uint8_t>() + ((size_t)c * kGrid3 + bi) * kEncCap);
+            it.qslot = (uint16_t)slot;
+            it.tau = (uint16_t)std::min(std::max(tau[c], 0), 65535);
+            it.pad = 0;
+        }
+    }
+    float *hq = L.h_misc.as<float>();
+    memcpy(hq, header_q, 4 * (size_t)nchunks);
+    if (!cuda_ok(cudaMemcpyAsync(L.enc_items.p, hi, sizeof(EncItem) * n, cudaMemcpyHostToDevice, L.stream), "H2D") ||
+        !cuda_ok(cudaMemcpyAsync(L.b_q.p, hq, 4 * (size_t)nchunks, cudaMemcpyHostToDevice, L.stream), "H2D") ||
+        !cuda_ok(cudaMemsetAsync(L.status.p, 0, 16, L.stream), "memset"))
+        return false;
+    EncParams ep;
+    ep.items = L.enc_items.as<EncItem>();
+    ep.n = (int)n;
+    ep.qtab = R->d_qtab;
+    ep.scan = R->d_scan;
+    ep.len = L.enc_len.as<uint32_t>();
+    ep.frac = L.enc_frac.as<uint8_t>();
+    ep.status = L.status.as<uint32_t>();
+    if (!cuda_ok(launch_encode(ep, L.stream), "encode launch")) return false;
+    BlobParams bp;
+    bp.nchunks = nchunks;
+    bp.payload = L.enc_pay.as<uint8_t>();
+    bp.len = L.enc_len.as<uint32_t>();
+    bp.frac = L.enc_frac.as<uint8_t>();
+    bp.header_q = L.b_q.as<float>();
+    bp.scratch = L.b_scratch.as<uint32_t>();
+    bp.lens16 = L.b_lens16.as<uint16_t>();
+    bp.bitmap = L.b_bitmap.as<uint8_t>();
+    bp.fmap = L.b_fmap.as<uint8_t>();
+    bp.fml = L.b_fml.as<uint32_t>();
+    bp.np = L.b_np.as<uint32_t>();
+    bp.blob_len = L.b_len.as<uint64_t>();
+    bp.blob_off = L.b_off.as<uint64_t>();
+    bp.blobs = nullptr;
+    if (!cuda_ok(launch_blob_layout(bp, L.stream), "blob layout launch")) return false;
+    uint64_t *hl = reinterpret_cast<uint64_t *>(L.h_misc.as<uint8_t>() + 8 * (size_t)nchunks);
+    uint32_t status = 0;
+    if (!cuda_ok(cudaMemcpyAsync(hl, L.b_len.p, 8 * (size_t)nchunks, cudaMemcpyDeviceToHost, L.stream), "D2H") ||
+        !cuda_ok(cudaMemcpyAsync(&status, L.status.p, 4, cudaMemcpyDeviceToHost, L.stream), "D2H") ||
+        !cuda_ok(cudaStreamSynchronize(L.stream), "encode sync"))
+        return false;
+    if (status) return set_error("block payload exceeded the encoder bound");
+    uint64_t total = 0;
+    for (int c = 0; c < nchunks; ++c) {
+        blob_len[c] = hl[c];
+        blob_off[c] = total;
+        total += (hl[c] + 15) & ~15ull;
+    }
+    uint64_t *ho = hl;   // reuse the staging for offsets
+    for (int c = 0; c < nchunks; ++c) ho[c] = blob_off[c];
+    if (!L.blobs.ensure(std::max<uint64_t>(total, 16))) return false;
+    bp.blobs = L.blobs.as<uint8_t>();
+    if (!cuda_ok(cudaMemcpyAsync(L.b_off.p, ho, 8 * (size_t)nchunks, cudaMemcpyHostToDevice, L.stream), "H2D") ||
+        !cuda_ok(launch_blob_fill(bp, L.stream), "blob fill launch") ||
+        !cuda_ok(launch_blob_hash(bp, L.stream), "blob hash launch") ||
+        !cuda_ok(cudaStreamSynchronize(L.stream), "blob sync"))
+        return false;
+    return true;
+}
+
+}  // namespace mcb

@@ -1,0 +1,99 @@
+// mcb_runtime.h -- device runtime behind the C ABI: lazy CUDA initialisation,
+// the per-quality table registry, per-thread streams and grow-only buffers, and
+// the decode / encode pipelines that feed the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "mcb_format.h"
+#include "mcb_kernels.h"
+
+namespace mcb {
+
+// Records the last error of the calling thread; returns false for chaining.
+bool set_error(const std::string &msg);
+bool cuda_ok(cudaError_t e, const char *what);
+const char *last_error();
+void clear_error();
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t n);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    ~DevBuf() { release(); }
+};
+// Grow-only pinned host buffer.
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t n);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    ~HostBuf() { release(); }
+};
+
+struct Runtime {
+    int device = -1;
+    int sms = 148;
+    uint16_t *d_scan = nullptr;   // scan position -> idx | band<<12
+    QTab *d_qtab = nullptr;       // kMaxQSlots tables
+    uint16_t h_scan[kN3];
+    float h_cos[16][16];
+    std::mutex qmu;
+    std::vector<uint64_t> qkeys; // (q bits << 32 | prior generation) per slot
+};
+
+// The process-wide runtime, initialised on first use. Null (with the thread's
+// error set) when no CUDA device is usable: the product has no CPU path.
+Runtime *runtime();
+// Device table slot for a (sanitised) quality under the active priors.
+int qslot(float q);
+
+// Device-side state of one batched decode: items, arena offsets, entropy
+// headers, arena and overflow pool. decode_prepare sizes the buffers for the
+// host item array and uploads items and offsets; decode_enqueue launches the
+// two stages (capturable into a CUDA graph).
+struct DecodeBatch {
+    DevBuf items, base, hdr, arena, pool, status;
+    int n = 0;
+    std::vector<std::pair<int, int>> subs;   // [i0, i1) ranges that fit the arena
+};
+// Per-thread execution resources: a stream and reusable buffers.
+struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    DevBuf status, out;
+    DecodeBatch batch;
+    DevBuf enc_items, enc_len, enc_frac, enc_pay, src;
+    DevBuf b_scratch, b_lens16, b_bitmap, b_fmap, b_fml, b_np, b_len, b_off, b_q, blobs;
+    HostBuf h_items, h_base, h_stage, h_misc;
+    LaunchCfg cfg;
+    ~Lane();
+};
+Lane *lane();
+
+bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s);
+bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s);
+
+// Decodes n items whose src/dst are device addresses (host-side item array),
+// enqueued on stream s (null: the lane's stream); false on a launch error.
+bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s = nullptr);
+
+// Encodes chunks of 256^3 voxels resident on the device (chunk c at
+// d_vox[c]) into assembled blobs. Synchronises; on return blob_len[c]
+// (0 = all air) and the blob offsets inside L.blobs are filled.
+bool encode_chunks(Lane &L, const uint8_t *const *d_vox, int nchunks, const float *header_q, const float *q,
+                   const int *tau, std::vector<uint64_t> &blob_off, std::vector<uint64_t> &blob_len);
+
+// Blocks whose corrupt streams were cut short during the last decode on the lane.
+uint32_t lane_bad_blocks(Lane &L);
+
+}  // namespace mcb

@@ -1,0 +1,340 @@
+"""ctypes binding of the matter-compressor C ABI.
+
+The same class binds the B200 library (libmc_b200.so beside this file) and,
+for the drop-in part of the ABI, any library exporting the reference's
+symbols, so one call sequence can be replayed against both. Pass
+``b200=False`` for a library without the mc_b200_* additions.
+
+The B200 library has no CPU path: `McLib.product()` raises when the library
+is missing or when no sm_100 device is usable.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmc_b200.so")
+CHUNK = 256 * 256 * 256
+
+
+class McBuf(C.Structure):
+    _fields_ = [("p", C.c_void_p), ("len", C.c_size_t), ("cap", C.c_size_t)]
+
+
+class McBox(C.Structure):
+    _fields_ = [("z0", C.c_long), ("y0", C.c_long), ("x0", C.c_long)]
+
+
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class McLib:
+    """Binding of one library; methods mirror the C entry points."""
+
+    def __init__(self, path, b200=True):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run __graft_entry__.build())")
+        self.path = path
+        self.L = L = C.CDLL(path)
+        self.b200 = b200
+        vp, u8p, i, f, u32, u64, sz, lg = (C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_uint32,
+                                            C.c_uint64, C.c_size_t, C.c_long)
+        sig = {
+            "mc_codec_init": (None, []),
+            "mc_codec_ctx_new": (vp, []),
+            "mc_codec_ctx_free": (None, [vp]),
+            "mc_codec_ctx_set_quality": (None, [vp, f]),
+            "mc_codec_ctx_get_quality": (f, [vp]),
+            "mc_codec_ctx_set_max_error": (None, [vp, i]),
+            "mc_codec_ctx_get_max_error": (i, [vp]),
+            "mc_apply_preset": (f, [vp, i]),
+            "mc_preset_quality": (f, [i]),
+            "mc_preset_tau": (i, [i]),
+            "mc_preset_name": (C.c_char_p, [i]),
+            "mc_codec_set_priors": (None, [vp, vp]),
+            "mc_enc_block": (i, [vp, u8p, C.POINTER(McBuf), C.POINTER(u32)]),
+            "mc_dec_block": (None, [vp, u8p, u32, u8p]),
+            "mc_enc_fracmap": (u32, [u8p, u8p, sz]),
+            "mc_dec_fracmap": (None, [u8p, u32, u8p]),
+            "mc_xxh64": (u64, [vp, sz, u64]),
+            "mc_archive_open": (vp, [C.c_char_p, i, f]),
+            "mc_archive_open_dims": (vp, [C.c_char_p, i, i, i, f]),
+            "mc_archive_close": (None, [vp]),
+            "mc_archive_chunk_offset": (u64, [vp, i, i, i, i]),
+            "mc_archive_chunk_coverage": (i, [vp, i, i, i, i]),
+            "mc_archive_data_len": (u64, [vp]),
+            "mc_archive_set_metadata": (i, [vp, vp, sz]),
+            "mc_archive_decode_block": (None, [vp, u64, i, i, i, u8p]),
+            "mc_archive_decode_chunk": (None, [vp, u64, u8p, i]),
+            "mc_archive_read_region": (None, [vp, i, lg, lg, lg, lg, lg, lg, u8p, sz, sz, i]),
+            "mc_archive_read_regions": (None, [vp, i, vp, i, lg, lg, lg, u8p, sz, i]),
+            "mc_archive_append_chunk_par": (i, [vp, i, i, i, i, u8p, f, i]),
+            "mc_archive_append_chunk_ctx": (i, [vp, vp, i, i, i, i, u8p]),
+            "mc_archive_append_chunk_raw": (i, [vp, i, i, i, i, u8p]),
+            "mc_archive_append_chunk_raw_q": (i, [vp, i, i, i, i, u8p, f]),
+            "mc_archive_append_chunk_compressed": (i, [vp, i, i, i, i, u8p, sz]),
+            "mc_archive_reserve_index": (i, [vp, i, i, i, i]),
+            "mc_archive_block_present": (i, [vp, i, i, i, i]),
+            "mc_archive_block_fraction": (f, [vp, i, i, i, i]),
+            "mc_archive_sample_boxes": (i, [vp, i, u64, i, lg, lg, lg, f, vp]),
+            "mc_archive_set_priors": (i, [vp, vp, vp]),
+            "mc_archive_block_blob": (i, [vp, u64, i, i, i, C.POINTER(C.c_void_p), C.POINTER(u32)]),
+            "mc_chunk_compute_hash": (u64, [u8p, u64]),
+            "mc_verify_archive": (lg, [u8p, sz, i]),
+        }
+        if b200:
+            sig.update({
+                "mc_b200_init": (i, []),
+                "mc_b200_last_error": (C.c_char_p, []),
+                "mc_b200_clear_error": (None, []),
+                "mc_b200_last_bad_blocks": (u32, []),
+                "mc_b200_decode_chunk_blobs": (i, [vp, vp, i, u8p, sz]),
+                "mc_b200_archive_sync": (i, [vp, C.POINTER(C.c_void_p), C.POINTER(u64)]),
+                "mc_b200_decode_chunks_dev": (i, [vp, vp, i, vp, sz, vp]),
+                "mc_b200_read_regions_dev": (i, [vp, i, vp, i, lg, lg, lg, vp, sz, vp]),
+                "mc_b200_plan_decode_chunks": (vp, [vp, vp, i, vp, sz]),
+                "mc_b200_plan_launch": (i, [vp, vp]),
+                "mc_b200_plan_info": (None, [vp, C.POINTER(i), C.POINTER(lg), C.POINTER(u64)]),
+                "mc_b200_plan_free": (None, [vp]),
+                "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
+            })
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+
+    # ------------------------------------------------------------ construction
+    @classmethod
+    def product(cls):
+        """The B200 library, checked to have a usable device."""
+        lib = cls(LIB_PATH, b200=True)
+        if lib.L.mc_b200_init() != 0:
+            raise RuntimeError("matter-compressor-b200: " + (lib.last_error() or "no usable GPU"))
+        return lib
+
+    def last_error(self):
+        e = self.L.mc_b200_last_error() if self.b200 else None
+        return e.decode() if e else None
+
+    def check(self):
+        if self.b200:
+            e = self.last_error()
+            if e:
+                self.L.mc_b200_clear_error()
+                raise RuntimeError("matter-compressor-b200: " + e)
+
+    # ------------------------------------------------------------ codec
+    def ctx(self, q=8.0, tau=0):
+        c = self.L.mc_codec_ctx_new()
+        self.L.mc_codec_ctx_set_quality(c, q)
+        self.L.mc_codec_ctx_set_max_error(c, tau)
+        return c
+
+    def enc_block(self, vox, q, tau=0):
+        vox = np.ascontiguousarray(vox, dtype=np.uint8).reshape(-1)
+        c = self.ctx(q, tau)
+        buf = McBuf()
+        n = C.c_uint32(0)
+        coded = self.L.mc_enc_block(c, _ptr(vox), C.byref(buf), C.byref(n))
+        out = C.string_at(buf.p, n.value) if coded else b""
+        if buf.p:
+            _libc.free(buf.p)
+        self.L.mc_codec_ctx_free(c)
+        self.check()
+        return out
+
+    def dec_block(self, payload, q):
+        c = self.ctx(q)
+        dst = np.zeros(4096, np.uint8)
+        src = np.frombuffer(payload, np.uint8) if payload else np.zeros(1, np.uint8)
+        src = np.ascontiguousarray(src)
+        self.L.mc_dec_block(c, _ptr(src), len(payload), _ptr(dst))
+        self.L.mc_codec_ctx_free(c)
+        self.check()
+        return dst
+
+    def set_priors(self, plo, phi):
+        if plo is None:
+            self.L.mc_codec_set_priors(None, None)
+        else:
+            plo = np.ascontiguousarray(plo, np.uint16)
+            phi = np.ascontiguousarray(phi, np.uint16)
+            self.L.mc_codec_set_priors(_ptr(plo), _ptr(phi))
+
+    # ------------------------------------------------------------ archive
+    def open(self, path, nx, ny=None, nz=None, q=6.0):
+        a = self.L.mc_archive_open_dims(str(path).encode(), nx, ny or nx, nz or nx, q)
+        if not a:
+            raise RuntimeError(f"mc_archive_open_dims({path}) failed")
+        return Archive(self, a)
+
+
+class Archive:
+    """One open archive handle of a bound library."""
+
+    def __init__(self, lib, handle):
+        self.lib, self.a, self.L = lib, handle, lib.L
+
+    def close(self):
+        if self.a:
+            self.L.mc_archive_close(self.a)
+            self.a = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def chunk_offset(self, lod, cz, cy, cx):
+        return self.L.mc_archive_chunk_offset(self.a, lod, cz, cy, cx)
+
+    def append_par(self, lod, cz, cy, cx, vox, q, nthreads=0):
+        vox = np.ascontiguousarray(vox, np.uint8)
+        assert vox.size == CHUNK
+        rc = self.L.mc_archive_append_chunk_par(self.a, lod, cz, cy, cx, _ptr(vox), q, nthreads)
+        self.lib.check()
+        return rc
+
+    def append_ctx(self, lod, cz, cy, cx, vox, q, tau=0, preset=None):
+        vox = np.ascontiguousarray(vox, np.uint8)
+        c = self.lib.ctx(q, tau)
+        if preset is not None:
+            self.L.mc_apply_preset(c, preset)
+        rc = self.L.mc_archive_append_chunk_ctx(self.a, c, lod, cz, cy, cx, _ptr(vox))
+        self.L.mc_codec_ctx_free(c)
+        self.lib.check()
+        return rc
+
+    def decode_block(self, co, bz, by, bx):
+        dst = np.zeros(4096, np.uint8)
+        self.L.mc_archive_decode_block(self.a, co, bz, by, bx, _ptr(dst))
+        self.lib.check()
+        return dst
+
+    def decode_chunk(self, co, out=None, nthreads=0):
+        if out is None:
+            out = np.empty(CHUNK, np.uint8)
+        self.L.mc_archive_decode_chunk(self.a, co, _ptr(out), nthreads)
+        self.lib.check()
+        return out
+
+    def read_region(self, lod, z0, y0, x0, dz, dy, dx, out=None, sz=None, sy=None, nthreads=0):
+        sy = dx if sy is None else sy
+        sz = dy * sy if sz is None else sz
+        if out is None:
+            out = np.zeros(sz * dz, np.uint8)
+        self.L.mc_archive_read_region(self.a, lod, z0, y0, x0, dz, dy, dx, _ptr(out), sz, sy, nthreads)
+        self.lib.check()
+        return out
+
+    def read_regions(self, lod, boxes, dz, dy, dx, batch_stride=None, nthreads=0):
+        n = len(boxes)
+        arr = (McBox * n)(*[McBox(*b) for b in boxes])
+        crop = dz * dy * dx
+        stride = crop if batch_stride is None else batch_stride
+        out = np.zeros(stride * (n - 1) + crop, np.uint8)
+        self.L.mc_archive_read_regions(self.a, lod, C.cast(arr, C.c_void_p), n, dz, dy, dx, _ptr(out), stride,
+                                       nthreads)
+        self.lib.check()
+        return out
+
+    def sample_boxes(self, lod, seed, count, dz, dy, dx, min_frac):
+        arr = (McBox * count)()
+        got = self.L.mc_archive_sample_boxes(self.a, lod, seed, count, dz, dy, dx, min_frac, C.cast(arr, C.c_void_p))
+        return [(b.z0, b.y0, b.x0) for b in arr[:got]]
+
+    def block_blob(self, co, bz, by, bx):
+        p = C.c_void_p()
+        n = C.c_uint32()
+        if not self.L.mc_archive_block_blob(self.a, co, bz, by, bx, C.byref(p), C.byref(n)):
+            return b""
+        return C.string_at(p, n.value)
+
+    # ---- B200 additions ----
+    def append_chunks(self, lod, coords, vox_list, q, ctx_q=None, ctx_tau=0, on_device=False):
+        n = len(coords)
+        cc = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1))
+        if on_device:
+            ptrs = (C.c_void_p * n)(*[v for v in vox_list])
+        else:
+            keep = [np.ascontiguousarray(v, np.uint8) for v in vox_list]
+            ptrs = (C.c_void_p * n)(*[k.ctypes.data for k in keep])
+        c = self.lib.ctx(ctx_q, ctx_tau) if ctx_q is not None else None
+        rc = self.L.mc_b200_append_chunks(self.a, c, lod, _ptr(cc), n, C.cast(ptrs, C.c_void_p), int(on_device), q)
+        if c:
+            self.L.mc_codec_ctx_free(c)
+        self.lib.check()
+        return rc
+
+    def sync_device(self):
+        base = C.c_void_p()
+        n = C.c_uint64()
+        rc = self.L.mc_b200_archive_sync(self.a, C.byref(base), C.byref(n))
+        self.lib.check()
+        return rc, base.value, n.value
+
+    def decode_chunks_dev(self, offs, d_out, stride=CHUNK, stream=None):
+        o = np.ascontiguousarray(np.asarray(offs, np.uint64))
+        rc = self.L.mc_b200_decode_chunks_dev(self.a, _ptr(o), len(o), C.c_void_p(d_out), stride,
+                                              C.c_void_p(stream) if stream else None)
+        self.lib.check()
+        return rc
+
+    def read_regions_dev(self, lod, boxes, dz, dy, dx, d_out, batch_stride=None, stream=None):
+        n = len(boxes)
+        arr = (McBox * n)(*[McBox(*b) for b in boxes])
+        stride = dz * dy * dx if batch_stride is None else batch_stride
+        rc = self.L.mc_b200_read_regions_dev(self.a, lod, C.cast(arr, C.c_void_p), n, dz, dy, dx,
+                                             C.c_void_p(d_out), stride, C.c_void_p(stream) if stream else None)
+        self.lib.check()
+        return rc
+
+    def plan_chunks(self, offs, d_out, stride=CHUNK):
+        o = np.ascontiguousarray(np.asarray(offs, np.uint64))
+        p = self.L.mc_b200_plan_decode_chunks(self.a, _ptr(o), len(o), C.c_void_p(d_out), stride)
+        self.lib.check()
+        if not p:
+            raise RuntimeError("plan build failed")
+        return Plan(self.lib, p)
+
+
+class Plan:
+    def __init__(self, lib, handle):
+        self.lib, self.p = lib, handle
+
+    def launch(self, stream=None):
+        rc = self.lib.L.mc_b200_plan_launch(self.p, C.c_void_p(stream) if stream else None)
+        self.lib.check()
+        return rc
+
+    def info(self):
+        n, b, pb = C.c_int(), C.c_long(), C.c_uint64()
+        self.lib.L.mc_b200_plan_info(self.p, C.byref(n), C.byref(b), C.byref(pb))
+        return n.value, b.value, pb.value
+
+    def free(self):
+        if self.p:
+            self.lib.L.mc_b200_plan_free(self.p)
+            self.p = None
+
+
+def decode_chunk_blobs(lib, blobs, out=None):
+    """mc_b200_decode_chunk_blobs over a list of bytes/ndarray blobs (host in, host out)."""
+    n = len(blobs)
+    arrs = [np.frombuffer(b, np.uint8) if isinstance(b, (bytes, bytearray)) else b for b in blobs]
+    ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+    lens = np.asarray([a.size for a in arrs], np.uint64)
+    if out is None:
+        out = np.empty(n * CHUNK, np.uint8)
+    rc = lib.L.mc_b200_decode_chunk_blobs(C.cast(ptrs, C.c_void_p), _ptr(lens), n, _ptr(out), CHUNK)
+    lib.check()
+    if rc:
+        raise RuntimeError("mc_b200_decode_chunk_blobs failed")
+    return out

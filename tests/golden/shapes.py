@@ -1,0 +1,98 @@
+"""Deterministic integer-formula inputs for the golden vectors and tests.
+
+Every pattern is computed from index arithmetic only (no RNG streams), so the
+same bytes come out on every machine and numpy version.
+"""
+import numpy as np
+
+_Z, _Y, _X = np.meshgrid(np.arange(16), np.arange(16), np.arange(16), indexing="ij")
+
+
+def _hash_u8(i, salt):
+    h = (i.astype(np.uint64) * np.uint64(2654435761) + np.uint64(salt) * np.uint64(40503)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(15)
+    h = (h * np.uint64(2246822519)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(13)
+    return (h & np.uint64(0xFF)).astype(np.int64)
+
+
+def block_patterns():
+    """16^3 blocks covering the codec's paths: smooth, textured, noisy, mixed
+    air/material, sparse, constant, saturated, single voxel."""
+    i = np.arange(4096)
+    z, y, x = _Z.ravel(), _Y.ravel(), _X.ravel()
+    pats = []
+    pats.append(40 + ((x * 7 + y * 3 + z * 5) % 160))                        # sawtooth texture
+    pats.append(128 + 60 * np.sin(x * 0.3) * np.cos(y * 0.2) + 20 * np.cos(z * 0.45))   # smooth
+    pats.append(_hash_u8(i, 1))                                            # white noise
+    r = np.sqrt((x - 8.0) ** 2 + (y - 8.0) ** 2 + (z - 8.0) ** 2)
+    pats.append(np.where(r < 6, 120 + (i % 80), 0))                       # ball in air
+    pats.append(np.where(_hash_u8(i, 2) < 100, 0, 40 + _hash_u8(i, 3) % 180))   # 40% speckled air
+    pats.append(np.full(4096, 77))                                         # constant
+    pats.append(np.where((x + y + z) % 2 == 0, 255, 0))                  # checkerboard extremes
+    pats.append(np.where(i == 1234, 200, 0))                               # single voxel
+    pats.append(100 + 2 * x + 3 * y + 4 * z + (_hash_u8(i, 4) % 13))    # ramp + noise
+    pats.append(np.where(z < 8, 30 + (i % 170), 0))                       # half air
+    return [np.clip(p, 0, 255).astype(np.uint8) for p in pats]
+
+
+def frac_pattern(t):
+    i = np.arange(4096)
+    if t == 0:
+        return np.zeros(4096, np.uint8)
+    if t == 1:
+        return np.full(4096, 15, np.uint8)
+    if t == 2:
+        return (i % 16).astype(np.uint8)
+    if t == 3:
+        return (_hash_u8(i, 9) % 16).astype(np.uint8)
+    if t == 4:
+        return np.where(i < 2048, 15, np.where(i % 7 == 0, 3, 0)).astype(np.uint8)
+    return ((i // 64) % 16).astype(np.uint8)
+
+
+def chunk_source(name):
+    """256^3 chunk from a reference-test style formula (z,y,x raster)."""
+    z, y, x = np.meshgrid(np.arange(256), np.arange(256), np.arange(256), indexing="ij", sparse=True)
+    if name == "ball":        # the reference roundtrip test's ball, q=8 style
+        r = np.sqrt((x - 128.0) ** 2 + (y - 128.0) ** 2 + (z - 128.0) ** 2)
+        v = 128.0 + 100.0 * np.cos(r * 0.15)
+        v = np.clip(v, 1, 255)
+        out = np.where(r > 256 * 0.4, 0, np.floor(v))
+    elif name == "sphere_tex":  # textured sphere, coarse texture
+        d2 = (x - 128) ** 2 + (y - 128) ** 2 + (z - 128) ** 2
+        out = np.where(d2 > 120 * 120, 0, 60 + ((x // 4 * 7 + y // 4 * 3 + z // 4 * 5) % 120))
+    elif name == "half_air":
+        out = np.where(z < 128, 40 + ((x + y + z) % 150), 0) + 0 * (x + y)
+    elif name == "air":
+        out = np.zeros((256, 256, 256))
+    elif name == "waves":
+        out = 120 + 50 * np.sin(x * 0.05 + y * 0.03) * np.cos(z * 0.04) + 20 * np.sin(x * 0.2)
+        out = out + 0 * (x + y + z)
+    else:
+        raise KeyError(name)
+    return np.ascontiguousarray(np.broadcast_to(np.clip(out, 0, 255), (256, 256, 256)).astype(np.uint8))
+
+
+def archive_sequence():
+    """A fixed append sequence into a 512x256x256 archive (two LOD0 chunks,
+    then preset-ladder chunks at reused coordinates, an air chunk)."""
+    return [
+        {"name": "ball_par_q8", "op": "par", "at": (0, 0, 0), "q": 8.0, "src": "ball"},
+        {"name": "waves_par_q3", "op": "par", "at": (0, 0, 1), "q": 3.0, "src": "waves"},
+        {"name": "tex_preset4", "op": "ctx", "at": (1, 0, 0), "preset": 4, "src": "sphere_tex"},
+        {"name": "half_preset2", "op": "ctx", "at": (1, 1, 1), "preset": 2, "src": "half_air"},
+        {"name": "air_ctx", "op": "ctx", "at": (2, 0, 0), "preset": 4, "src": "air"},
+        {"name": "air_par", "op": "par", "at": (2, 0, 1), "q": 6.0, "src": "air"},
+        {"name": "waves_preset7", "op": "ctx", "at": (3, 3, 3), "preset": 7, "src": "waves"},
+    ]
+
+
+def blob_len(data, co):
+    """Total length of the chunk blob at file offset co: header, fmap,
+    bitmap, one u16 length per present block, payloads."""
+    fml = int.from_bytes(data[co + 12:co + 14], "little")
+    bm = np.frombuffer(data, np.uint8, 512, co + 14 + fml)
+    npres = int(np.unpackbits(bm).sum())
+    lens = np.frombuffer(data, np.uint16, npres, co + 14 + fml + 512)
+    return 14 + fml + 512 + 2 * npres + int(lens.astype(np.int64).sum())

@@ -1,0 +1,185 @@
+"""GPU parity through the C ABI: the CUDA codec against the golden vectors
+(reference output), the oracle and -- where shipped -- the reference build.
+Integer/byte results must be bit-exact."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import shapes
+from conftest import ctx_q, sha
+
+pytestmark = pytest.mark.gpu
+CHUNK = 256 ** 3
+PRESETS = [(0.5, 1), (0.5, 2), (1.0, 4), (2.5, 8), (6.0, 16), (16.0, 32), (32.0, 64), (64.0, 128)]
+
+
+def test_block_decode_golden(gpu, golden_blocks):
+    g = golden_blocks
+    for i in range(len(g["q"])):
+        p = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        if not p:
+            continue
+        assert sha(gpu.dec_block(p, ctx_q(float(g["q"][i])))) == g["decoded_sha"][i], f"case {i}"
+
+
+def test_block_encode_golden(gpu, golden_blocks):
+    g = golden_blocks
+    pats = shapes.block_patterns()
+    for i in range(len(g["q"])):
+        want = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        got = gpu.enc_block(pats[int(g["kind"][i])], float(g["q"][i]), int(g["tau"][i]))
+        assert got == want, f"case {i}: kind {int(g['kind'][i])} q={float(g['q'][i])} tau={int(g['tau'][i])}"
+
+
+def test_corrupt_streams_golden(gpu, golden_corrupt):
+    g = golden_corrupt
+    for i in range(len(g["q"])):
+        p = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        assert sha(gpu.dec_block(p, float(g["q"][i]))) == g["decoded_sha"][i], f"stream {i}"
+    assert gpu.L.mc_b200_last_bad_blocks() == 0
+
+
+def test_chunk_blobs_decode_golden(gpu, golden_chunks):
+    from mcb200 import decode_chunk_blobs
+    g = golden_chunks
+    blobs = [g["blobs"][g["offs"][i]:g["offs"][i + 1]] for i in range(len(g["offs"]) - 1)]
+    out = decode_chunk_blobs(gpu, [b if b.size else None for b in blobs] if False else blobs)
+    for i in range(len(blobs)):
+        assert sha(out[i * CHUNK:(i + 1) * CHUNK]) == g["decoded_sha"][i], g["names"][i]
+
+
+def _append_sequence(lib, path):
+    offs = []
+    with lib.open(path, 1024, 1024, 1024, 6.0) as a:
+        for st in shapes.archive_sequence():
+            vox = shapes.chunk_source(st["src"])
+            if st["op"] == "par":
+                assert a.append_par(0, *st["at"], vox, st["q"]) == 0
+            else:
+                assert a.append_ctx(0, *st["at"], vox, 8.0, preset=st["preset"]) == 0
+            offs.append(a.chunk_offset(0, *st["at"]))
+        lib.L.mc_archive_set_metadata(a.a, b"golden", 6)
+    return open(path, "rb").read(), offs
+
+
+def test_archive_byte_identical(gpu, golden_chunks, tmp_path):
+    data, offs = _append_sequence(gpu, str(tmp_path / "g.mca"))
+    g = golden_chunks
+    assert len(data) == int(g["archive_len"])
+    assert hashlib.sha256(data).hexdigest() == str(g["archive_sha"])
+
+
+def test_archive_decode_paths(gpu, golden_chunks, tmp_path):
+    """decode_chunk, per-block decode_block, read_region(s) on a GPU-built archive."""
+    g = golden_chunks
+    path = str(tmp_path / "d.mca")
+    _, offs = _append_sequence(gpu, path)
+    with gpu.open(path, 1024, 1024, 1024, 6.0) as a:
+        for i, co in enumerate(offs):
+            assert sha(a.decode_chunk(co)) == g["decoded_sha"][i], g["names"][i]
+        co = offs[0]
+        whole = a.decode_chunk(co).reshape(256, 256, 256)
+        for bz, by, bx in [(0, 0, 0), (8, 8, 8), (15, 15, 15), (3, 12, 7), (12, 3, 9)]:
+            blk = a.decode_block(co, bz, by, bx).reshape(16, 16, 16)
+            assert np.array_equal(blk, whole[bz * 16:bz * 16 + 16, by * 16:by * 16 + 16, bx * 16:bx * 16 + 16])
+        # region == crop of the decoded chunk (reference v6 test, section 5)
+        reg = a.read_region(0, 10, 20, 30, 64, 64, 64).reshape(64, 64, 64)
+        assert np.array_equal(reg, whole[10:74, 20:84, 30:94])
+        # strided region output leaves the gaps untouched
+        out = np.full(70 * 80 * 40, 0xAB, np.uint8)
+        a.read_region(0, 100, 5, 250, 40, 30, 20, out=out, sz=80 * 70, sy=70)
+        o = out.reshape(40, 80, 70)
+        w1 = a.decode_chunk(a.chunk_offset(0, 0, 0, 1)).reshape(256, 256, 256)
+        want = np.concatenate([whole[100:140, 5:35, 250:256], w1[100:140, 5:35, 0:14]], axis=2)
+        assert np.array_equal(o[:, :30, :20], want)
+        assert np.all(o[:, 30:, :] == 0xAB) and np.all(o[:, :30, 20:] == 0xAB)
+        # batch == per-region, boxes crossing into absent chunks and past the volume
+        boxes = [(0, 0, 0), (10, 20, 30), (60, 100, 3), (64, 64, 300), (-8, 250, 1000)]
+        batch = a.read_regions(0, boxes, 64, 64, 64).reshape(len(boxes), 64, 64, 64)
+        for i, (z0, y0, x0) in enumerate(boxes):
+            single = a.read_region(0, z0, y0, x0, 64, 64, 64).reshape(64, 64, 64)
+            assert np.array_equal(batch[i], single), boxes[i]
+        # absent chunk and the air sentinel decode to zeros
+        assert not a.decode_chunk(0).any()
+        assert not a.decode_chunk(1).any()
+
+
+def test_against_reference_build(gpu, ref, golden_chunks, tmp_path):
+    """Same calls on the reference build and the GPU library: same blocks."""
+    path = str(tmp_path / "r.mca")
+    _append_sequence(ref, path)
+    with ref.open(path, 1024, 1024, 1024, 6.0) as ra:
+        co = ra.chunk_offset(0, 0, 0, 1)
+        want = ra.decode_chunk(co)
+        wreg = ra.read_regions(0, [(5, 200, 200), (130, 7, 255)], 48, 48, 48)
+    with gpu.open(path, 1024, 1024, 1024, 6.0) as ga:   # the GPU library reads the reference's file
+        assert np.array_equal(ga.decode_chunk(co), want)
+        assert np.array_equal(ga.read_regions(0, [(5, 200, 200), (130, 7, 255)], 48, 48, 48), wreg)
+
+
+def test_synthetic_chunk_q6(gpu, oracle, tmp_path):
+    """One 256^3 chunk of the benchmark generator at q=6 (40% air): GPU
+    append_par blob == oracle blob; every block decoded per call == oracle."""
+    import torch
+    import volumes
+    vox = volumes.chunk(0, 0.4, device="cuda").cpu().numpy().reshape(-1)
+    want_blob = oracle.encode_chunk(vox, 6.0, 0)
+    with gpu.open(str(tmp_path / "s.mca"), 256, 256, 256, 6.0) as a:
+        assert a.append_par(0, 0, 0, 0, vox, 6.0) == 0
+        co = a.chunk_offset(0, 0, 0, 0)
+        got_blob = bytes(np.fromfile(str(tmp_path / "s.mca"), np.uint8)[co:co + len(want_blob)])
+        assert got_blob == want_blob
+        want = oracle.decode_chunk(want_blob).reshape(256, 256, 256)
+        got = a.decode_chunk(co).reshape(256, 256, 256)
+        assert np.array_equal(got, want)
+        for bi in range(0, 4096, 97):
+            bz, by, bx = bi >> 8, (bi >> 4) & 15, bi & 15
+            blk = a.decode_block(co, bz, by, bx).reshape(16, 16, 16)
+            assert np.array_equal(blk, want[bz * 16:bz * 16 + 16, by * 16:by * 16 + 16, bx * 16:bx * 16 + 16])
+        # device-output paths: decode_chunks_dev and a graph-captured plan
+        d_out = torch.empty(2 * CHUNK, dtype=torch.uint8, device="cuda")
+        assert a.decode_chunks_dev([co, 0], d_out.data_ptr()) == 0
+        assert np.array_equal(d_out[:CHUNK].cpu().numpy(), want.reshape(-1))
+        assert not d_out[CHUNK:].any().item()
+        d2 = torch.zeros(CHUNK, dtype=torch.uint8, device="cuda")
+        plan = a.plan_chunks([co], d2.data_ptr())
+        plan.launch()
+        torch.cuda.synchronize()
+        assert np.array_equal(d2.cpu().numpy(), want.reshape(-1))
+        launches, blocks, pbytes = plan.info()
+        assert blocks == 4096 and launches >= 2
+        plan.free()
+
+
+def test_mixed_quality_batch(gpu, oracle, tmp_path):
+    """Chunks of different q in one batched append and one batched decode."""
+    import torch
+    import volumes
+    qs = [1.0, 3.0, 6.0, 12.0]
+    vox = [volumes.region(7 + i, (0, 0, 256 * i), (256, 256, 256), 0.3, device="cuda").cpu().numpy() for i in range(4)]
+    with gpu.open(str(tmp_path / "m.mca"), 1024, 256, 256, 6.0) as a:
+        for i, q in enumerate(qs):
+            assert a.append_par(0, 0, 0, i, vox[i], q) == 0
+        offs = [a.chunk_offset(0, 0, 0, i) for i in range(4)]
+        d_out = torch.empty(4 * CHUNK, dtype=torch.uint8, device="cuda")
+        assert a.decode_chunks_dev(offs, d_out.data_ptr()) == 0
+        got = d_out.cpu().numpy()
+        data = np.fromfile(str(tmp_path / "m.mca"), np.uint8).tobytes()
+    for i, q in enumerate(qs):
+        blob = data[offs[i]:offs[i] + shapes.blob_len(data, offs[i])]
+        assert blob == oracle.encode_chunk(vox[i], q, 0), q
+        assert np.array_equal(got[i * CHUNK:(i + 1) * CHUNK], oracle.decode_chunk(blob)), q
+
+
+def test_preset_ladder_tau_bound(gpu, tmp_path):
+    """Preset ladder through append_chunk_ctx: |err| <= tau on every voxel."""
+    import volumes
+    vox = volumes.region(3, (0, 0, 0), (256, 256, 256), 0.3, device="cuda").cpu().numpy()
+    with gpu.open(str(tmp_path / "t.mca"), 256, 256, 256 * 8, 6.0) as a:
+        for lvl, (q, tau) in enumerate(PRESETS):
+            assert a.append_ctx(0, lvl, 0, 0, vox, 8.0, preset=lvl) == 0
+            dec = a.decode_chunk(a.chunk_offset(0, lvl, 0, 0)).reshape(vox.shape)
+            err = np.abs(dec.astype(int) - vox.astype(int))
+            assert err.max() <= tau, (lvl, err.max())

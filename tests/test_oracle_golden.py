@@ -1,0 +1,84 @@
+"""The oracle (our C restatement) reproduces the reference's golden vectors
+byte for byte: block payloads, decoded blocks, corrupt streams, fraction maps,
+XXH64, whole-chunk blobs and decoded chunks."""
+import numpy as np
+import pytest
+
+import shapes
+from conftest import ctx_q, sha
+
+
+def test_block_encode_decode(oracle, golden_blocks):
+    g = golden_blocks
+    pats = shapes.block_patterns()
+    for i in range(len(g["q"])):
+        q, tau, k = float(g["q"][i]), int(g["tau"][i]), int(g["kind"][i])
+        want = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        got = oracle.enc_block(pats[k], q, tau)
+        assert got == want, f"case {i}: pattern {k} q={q} tau={tau}"
+        dec = oracle.dec_block(got, ctx_q(q)) if got else np.zeros(4096, np.uint8)
+        assert sha(dec) == g["decoded_sha"][i], f"case {i} decode"
+
+
+def test_max_error_bound(oracle):
+    """|err| <= tau on every voxel when coded with a max-error bound
+    (the reference's api test: tau bound, air within [0, tau])."""
+    for k, vox in enumerate(shapes.block_patterns()):
+        for q, tau in [(2.0, 3), (6.0, 8), (0.5, 1), (16.0, 32)]:
+            p = oracle.enc_block(vox, q, tau)
+            if not p:
+                assert not vox.any()
+                continue
+            d = oracle.dec_block(p, q).astype(int)
+            assert np.abs(d - vox.astype(int)).max() <= tau, (k, q, tau)
+
+
+def test_corrupt_streams(oracle, golden_corrupt):
+    g = golden_corrupt
+    for i in range(len(g["q"])):
+        p = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        assert sha(oracle.dec_block(p, float(g["q"][i]))) == g["decoded_sha"][i], f"stream {i}"
+
+
+def test_fracmap_and_xxh64(oracle, golden_meta):
+    g = golden_meta
+    for t in range(len(g["frac"])):
+        want = g["fmap"][g["fmap_offs"][t]:g["fmap_offs"][t + 1]].tobytes()
+        assert oracle.enc_fracmap(g["frac"][t]) == want
+        assert np.array_equal(oracle.dec_fracmap(want), g["frac"][t])
+    data = g["xx_data"].tobytes()
+    for ln, seed, h in g["xx"]:
+        assert oracle.xxh64(data[:int(ln)], int(seed)) == int(h)
+
+
+def test_chunk_blobs(oracle, golden_chunks):
+    g = golden_chunks
+    steps = shapes.archive_sequence()
+    for i, st in enumerate(steps):
+        want = g["blobs"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        vox = shapes.chunk_source(st["src"])
+        if st["op"] == "par":
+            got = oracle.encode_chunk(vox, st["q"], 0)
+        else:
+            q, tau = [(0.5, 1), (0.5, 2), (1.0, 4), (2.5, 8), (6.0, 16), (16.0, 32), (32.0, 64), (64.0, 128)][st["preset"]]
+            got = oracle.encode_chunk(vox, q, tau)
+        assert got == want, st["name"]
+        if want:
+            assert oracle.blob_hash(want) == int.from_bytes(want[4:12], "little")
+            assert sha(oracle.decode_chunk(want)) == g["decoded_sha"][i], st["name"]
+
+
+def test_scan_and_priors(oracle):
+    scan = np.zeros(4096, np.uint16)
+    oracle.L.or_scan_table(scan.ctypes.data)
+    idx = scan.astype(int)
+    l1 = (idx >> 8) + ((idx >> 4) & 15) + (idx & 15)
+    assert sorted(idx.tolist()) == list(range(4096))
+    assert np.all(np.diff(l1) >= 0)
+    same = np.diff(l1) == 0
+    assert np.all(np.diff(idx)[same] > 0)      # ties in raster order
+    lo, hi = oracle.priors_for_q(1.0), oracle.priors_for_q(12.0)
+    assert lo[0] == 115 and hi[0] == 456        # SIG slot 0 endpoints
+    assert oracle.priors_for_q(0.25)[0] == 115  # q <= 1 uses the q=1 table
+    mid = oracle.priors_for_q(3.4641)           # log-midpoint lies between
+    assert min(lo[0], hi[0]) <= mid[0] <= max(lo[0], hi[0])
