@@ -167,8 +167,8 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
         return ms;
     };
     float best_ms = 1e30f;
-    const int ent_opts[] = {2, 3, 4, 5};
-    const int rec_opts[] = {3, 5, 7};
+    const int ent_opts[] = {4, 5, 6};
+    const int rec_opts[] = {3, 4, 5};
     for (int e : ent_opts) {
         LaunchCfg c = best;
         c.ent_ctas_per_sm = e;

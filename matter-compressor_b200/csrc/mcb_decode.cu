@@ -31,29 +31,69 @@ namespace mcb {
 __constant__ float c_cos[16][16];
 
 // ---------------------------------------------------------------- stage 1
+// Lane states. The first four cover almost every bin of a block and share one
+// branch-light step (header bins, EOB prefix, significance, magnitude rungs
+// with their sign); the rest (EOB suffix, Exp-Golomb tails and their signs,
+// corrections) take a slow path entered a few times per block.
 enum : uint32_t {
-    S_FLAG = 0, S_DC, S_EOBP, S_SIG, S_MAG,   // context-coded bins
-    S_EOBS, S_SIGN, S_EGP, S_EGS, S_CSIGN,    // bypass bins
-    S_DONE, S_IDLE
+    F_HDR = 0,   // 10 context bins: flag0, flag1, dc bits 7..0 (contexts 0..9)
+    F_EOBP,      // EOB bit-length prefix, context 10+k
+    F_SIG,       // significance of scan position p
+    F_MAG,       // unary magnitude rung k, context 56+k (a zero rung takes the sign too)
+    S_SIGN,      // sign bypass after an Exp-Golomb magnitude
+    S_EOBS,      // EOB bits below the MSB (bypass, k bits)
+    S_EGP,       // Exp-Golomb prefix (bypass)
+    S_EGS,       // Exp-Golomb suffix (bypass, rem bits, 16 at a time)
+    S_CSIGN,     // correction sign (bypass)
+    S_DONE,
+    S_IDLE
 };
 enum : uint32_t { R_MAG = 0, R_CCOUNT, R_CGAP, R_CMAG };
 
 struct LaneState {
     const uint8_t *src;
-    uint32_t len, pos, code, range;
-    uint32_t state, k, p, eob, hist;
-    uint32_t dc, flags;
-    int ez, ey, ex;
-    uint32_t mag, nbits, rem, acc, ret;
-    uint32_t nent, nnz, ncorr, ccount, cpos, cneg;
+    uint32_t len, rpos;        // payload length, next byte index the window loads
+    uint64_t wcur, wnext;      // byte window: current 8 bytes (wn left), next 8 bytes
+    uint32_t wn;
+    uint32_t code, range;
+    uint32_t st, k, lbase, p, eob, hist, hdr, mag;
+    uint32_t nbits, rem, acc, ret;
+    uint32_t ncorr, ccount, cpos, cneg;
+    uint32_t nent;             // entries written: coefficients, then 2 per correction
     uint64_t base;
     uint32_t cap, ovf, bad;
     int item;
 };
 
-__device__ __forceinline__ uint8_t fetch(LaneState &L) {
-    uint8_t b = 0;
-    if (L.pos < L.len) { b = __ldg(L.src + L.pos); L.pos++; }
+// Eight payload bytes from byte index pos (little-endian), zero past len.
+// Reads two aligned 8-byte words: every buffer that holds payloads keeps 64
+// readable bytes past its end and starts 256-byte aligned, so an aligned-down
+// address never precedes its buffer.
+__device__ __forceinline__ uint64_t load8(const uint8_t *src, uint32_t len, uint32_t pos) {
+    if (pos >= len) return 0ull;
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(src) + pos;
+    const uint64_t *a = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
+    const uint32_t sh = (uint32_t)(addr & 7) * 8u;
+    const uint64_t lo = __ldg(a), hi = __ldg(a + 1);
+    uint64_t w = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+    const uint32_t avail = len - pos;
+    if (avail < 8) w &= (1ull << (8 * avail)) - 1ull;
+    return w;
+}
+
+__device__ __forceinline__ void refill(LaneState &L) {
+    L.wcur = L.wnext;
+    L.wn = 8;
+    L.wnext = load8(L.src, L.len, L.rpos);
+    L.rpos += 8;
+}
+
+// The window always holds at least one unread byte: consuming the last one
+// refills it at once (invariant wn >= 1 between calls).
+__device__ __forceinline__ uint32_t next_byte(LaneState &L) {
+    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
+    L.wcur >>= 8;
+    if (--L.wn == 0) refill(L);
     return b;
 }
 
@@ -61,11 +101,11 @@ __device__ __forceinline__ void put_entry(LaneState &L, const EntParams &P, uint
     uint32_t j = L.nent;
     if (j < L.cap) {
         P.arena[L.base + j] = v;
-    } else {
+    } else {   // only corrupt streams get here
         if (L.ovf == 0xFFFFFFFFu) {
             uint32_t need = kEntryMax - L.cap;
             uint32_t off = atomicAdd(P.pool_used, need);
-            if ((uint64_t)off + need > P.pool_cap) { L.bad = 1; L.state = S_DONE; return; }
+            if ((uint64_t)off + need > P.pool_cap) { L.bad = 1; L.st = S_DONE; return; }
             L.ovf = off;
         }
         P.pool[L.ovf + (j - L.cap)] = v;
@@ -73,228 +113,305 @@ __device__ __forceinline__ void put_entry(LaneState &L, const EntParams &P, uint
     L.nent = j + 1;
 }
 
-__device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uint32_t *ctx, int slot) {
-    L.item = slot;
+struct NextItem {   // descriptor of the lane's next block, loaded ahead of need
+    int slot;
+    uint64_t src, base;
+    uint32_t len, qslot;
+};
+
+__device__ __forceinline__ void prefetch_item(NextItem &N, const EntParams &P, int idx) {
+    N.slot = -1;
+    if (idx >= P.n) return;
+    const int slot = P.order ? (int)P.order[idx] : idx;
     const DecItem &it = P.items[slot];
-    L.src = reinterpret_cast<const uint8_t *>(it.src);
-    L.len = it.len;
-    L.pos = 0;
-    L.base = P.base[slot];
-    L.cap = entry_cap(it.len);
+    N.slot = slot;
+    N.src = it.src;
+    N.len = it.len;
+    N.qslot = it.qslot;
+    N.base = P.base[slot];
+}
+
+__device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uint16_t *ctx, const NextItem &N) {
+    L.item = N.slot;
+    L.src = reinterpret_cast<const uint8_t *>(N.src);
+    L.len = N.len;
+    L.base = N.base;
+    L.cap = entry_cap(N.len);
     L.ovf = 0xFFFFFFFFu;
     L.bad = 0;
-    L.nent = 0; L.nnz = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
-    L.ez = L.ey = L.ex = -1;
-    L.dc = 0; L.flags = 0;
-    L.k = 0; L.p = 0; L.eob = 0; L.hist = 0; L.mag = 0;
+    L.nent = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
+    L.hdr = 0;
+    L.k = 0; L.lbase = kCtxFlag; L.p = 0; L.eob = 0; L.hist = 0; L.mag = 0;
     L.nbits = 0; L.rem = 0; L.acc = 0; L.ret = 0;
-    if (it.len == 0) { L.state = S_DONE; return; }   // absent block: zeros
-    const QTab &qt = P.qtab[it.qslot];
-    for (int j = 0; j < kNumCtx; ++j) ctx[j * 32] = qt.ctx[j];
+    if (N.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
+    const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[N.qslot].ctx);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {               // 72 u16 initial contexts
+        uint4 v = __ldg(q + j);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int c = j * 8 + h * 2;
+            if (c < kNumCtx) ctx[c * 32] = (uint16_t)w[h];
+            if (c + 1 < kNumCtx) ctx[(c + 1) * 32] = (uint16_t)(w[h] >> 16);
+        }
+    }
+    L.wcur = load8(L.src, L.len, 0);
+    L.wnext = load8(L.src, L.len, 8);
+    L.wn = 8;
+    L.rpos = 16;
     L.range = 0xFFFFFFFFu;
     L.code = 0;
-    for (int i = 0; i < 5; ++i) L.code = (L.code << 8) | fetch(L);
-    L.state = S_FLAG;
+    for (int i = 0; i < 5; ++i) L.code = (L.code << 8) | next_byte(L);
+    L.st = F_HDR;
 }
 
 __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
     EntHdr h;
-    h.dc = (uint8_t)L.dc;
-    h.flags = (uint8_t)L.flags;
+    h.dc = (uint8_t)(L.hdr & 0xFF);
+    h.flags = (uint8_t)(((L.hdr >> 9) & 1) | (((L.hdr >> 8) & 1) << 1));
     h.bad = (uint8_t)L.bad;
     h.pad = 0;
-    h.ez = (int8_t)L.ez; h.ey = (int8_t)L.ey; h.ex = (int8_t)L.ex; h.pad2 = 0;
-    h.nnz = (uint16_t)L.nnz;
+    h.ez = h.ey = h.ex = -1;    // extents are taken from the entries by k_reconstruct
+    h.pad2 = 0;
+    h.nnz = (uint16_t)(L.nent - 2 * L.ccount);
     h.ncorr = (uint16_t)L.ccount;
     h.ovf = L.ovf;
     P.hdr[L.item] = h;
     if (L.bad) atomicAdd(P.status, 1u);
 }
 
-// Position p of the coefficient scan becomes current: the last position is
-// significant by definition and costs no bin (src/mc_codec.c:364).
+// flags bit 1 (has corrections) is the second header bin
+__device__ __forceinline__ bool has_corr(const LaneState &L) { return (L.hdr >> 8) & 1; }
+
+// Scan position p became current: past the end -> corrections or done; the
+// last position is significant by definition and costs no bin
+// (src/mc_codec.c:364).
 __device__ __forceinline__ void goto_position(LaneState &L) {
     if (L.p >= L.eob) {
-        if (L.flags & 2) { L.state = S_EGP; L.nbits = 0; L.ret = R_CCOUNT; }
-        else L.state = S_DONE;
+        if (has_corr(L)) { L.st = S_EGP; L.nbits = 0; L.ret = R_CCOUNT; }
+        else L.st = S_DONE;
     } else if (L.p == L.eob - 1) {
         L.hist = (L.hist << 1) | 1u;
-        L.state = S_MAG; L.k = 0;
+        L.st = F_MAG;
+        L.k = 0;
+        L.lbase = kCtxMag;
     } else {
-        L.state = S_SIG;
+        L.st = F_SIG;
     }
 }
 
-__device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, const uint16_t *scan, uint32_t val) {
+__device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint32_t val) {
     switch (L.ret) {
     case R_MAG:
         L.mag = 12u + val;            // 11 unary rungs + Exp-Golomb tail + 1
-        L.state = S_SIGN;
+        L.st = S_SIGN;                // the sign bypass follows
         break;
     case R_CCOUNT: {
         uint32_t n = val + 1u;
         if (n > (uint32_t)kN3) n = kN3;
         L.ncorr = n; L.ccount = 0; L.cpos = 0;
-        if (n == 0) L.state = S_DONE;
-        else { L.state = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
+        if (n == 0) L.st = S_DONE;
+        else { L.st = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
         break;
     }
     case R_CGAP:
         L.cpos += val;
-        L.state = S_CSIGN;
+        L.st = S_CSIGN;
         break;
     default: {   // R_CMAG
         uint32_t m = val + 1u;
-        if (L.cpos >= (uint32_t)kN3) { L.state = S_DONE; break; }
+        if (L.cpos >= (uint32_t)kN3) { L.st = S_DONE; break; }
         put_entry(L, P, L.cpos);
-        if (L.state == S_DONE) break;
+        if (L.st == S_DONE) break;
         put_entry(L, P, L.cneg ? 0u - m : m);
-        if (L.state == S_DONE) break;
+        if (L.st == S_DONE) break;
         L.ccount++;
-        if (L.ccount == L.ncorr) L.state = S_DONE;
-        else { L.state = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
+        if (L.ccount == L.ncorr) L.st = S_DONE;
+        else { L.st = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
         break;
     }
     }
 }
 
+// Slow path: one bypass step of the rare states (src/mc_codec.c:205,216-238).
+__device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P, const uint32_t *s_scan) {
+    const uint32_t st = L.st;
+    const uint32_t nb = st == S_EOBS ? L.k : (st == S_EGS ? min(L.rem, 16u) : 1u);
+    L.range >>= nb;
+    uint32_t q;
+    if (nb == 1) {
+        q = L.code >= L.range ? 1u : 0u;
+    } else {
+        q = L.code / L.range;
+        const uint32_t mx = (1u << nb) - 1u;
+        q = q > mx ? mx : q;
+    }
+    L.code -= q * L.range;
+    while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
+    switch (st) {
+    case S_EOBS:
+        L.eob = (1u << L.k) | q;
+        if (L.eob > (uint32_t)kN3) L.eob = kN3;
+        L.p = 0;
+        L.hist = 0;
+        goto_position(L);
+        break;
+    case S_EGP:   // Exp-Golomb prefix: count one-bits, capped on corrupt streams
+        if (q) {
+            if (++L.nbits >= (uint32_t)kEgCap) { L.bad = 1; L.st = S_DONE; }
+        } else if (L.nbits == 0) {
+            eg_return(L, P, 0);
+        } else {
+            L.st = S_EGS; L.rem = L.nbits; L.acc = 0;
+        }
+        break;
+    case S_EGS:
+        L.acc = (L.acc << nb) | q;
+        L.rem -= nb;
+        if (L.rem == 0) eg_return(L, P, ((1u << (L.nbits & 31)) | L.acc) - 1u);
+        break;
+    case S_SIGN: {
+        const uint32_t m = L.mag;
+        put_entry(L, P, (s_scan[L.p] & 0xFFFu) | ((q ? 0u - m : m) << 16));
+        if (L.st != S_DONE) { L.p++; goto_position(L); }
+        break;
+    }
+    default:      // S_CSIGN
+        L.cneg = q;
+        L.st = S_EGP; L.nbits = 0; L.ret = R_CMAG;
+        break;
+    }
+}
+
+// Renormalise after a bin: one byte by selects (the window always holds one),
+// further bytes (rare: extreme p0) by the loop (src/mc_codec.c:202).
+__device__ __forceinline__ void renorm(LaneState &L) {
+    const bool need = L.range < (1u << 24);
+    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
+    L.code = need ? (L.code << 8) | b : L.code;
+    L.range = need ? L.range << 8 : L.range;
+    L.wcur = need ? L.wcur >> 8 : L.wcur;
+    L.wn -= need ? 1u : 0u;
+    if (L.wn == 0) refill(L);
+    while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
+}
+
+// Scan position p became current (fast-path variant of goto_position).
+__device__ __forceinline__ void advance(LaneState &L) {
+    const uint32_t p = L.p;
+    const bool past = p >= L.eob;
+    const bool last = !past && p + 1 == L.eob;      // significant by definition (src/mc_codec.c:364)
+    L.hist = last ? (L.hist << 1) | 1u : L.hist;
+    L.k = 0;
+    L.lbase = kCtxMag;
+    L.nbits = 0;
+    L.ret = R_CCOUNT;
+    L.st = past ? (has_corr(L) ? (uint32_t)S_EGP : (uint32_t)S_DONE) : (last ? (uint32_t)F_MAG : (uint32_t)F_SIG);
+}
+
+// One context-coded bin of a lane in a fast state (src/mc_codec.c:198-204):
+// F_SIG uses the significance context of its scan position, the ladders
+// (header, EOB prefix, magnitude rungs) context lbase + k. A magnitude ended
+// by a zero rung takes its sign bypass bit in the same step.
+__device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint16_t *ctx, const uint32_t *s_scan) {
+    const uint32_t st = L.st;
+    const bool is_sig = st == F_SIG;
+    const uint32_t sc = s_scan[L.p];                 // idx | (24 + 4*band) << 12
+    const uint32_t dens = min(__popc(L.hist & 0xFFFFu), 3);
+    const uint32_t cidx = is_sig ? (sc >> 12) + dens : L.lbase + L.k;
+    uint32_t p0 = ctx[cidx * 32];
+    const uint32_t r0 = (L.range >> 12) * p0;
+    const uint32_t bit = L.code >= r0 ? 1u : 0u;
+    L.code -= bit ? r0 : 0u;
+    L.range = bit ? L.range - r0 : r0;
+    ctx[cidx * 32] = (uint16_t)(bit ? p0 - (p0 >> 4) : p0 + ((4096u - p0) >> 4));
+    renorm(L);
+
+    if (is_sig) {
+        L.hist = (L.hist << 1) | bit;
+        if (bit) { L.st = F_MAG; L.k = 0; L.lbase = kCtxMag; }
+        else { L.p++; advance(L); }
+    } else if (st == F_MAG) {                        // 12 adaptive unary rungs (src/mc_codec.c:268-275)
+        if (bit) {
+            if (L.k < 11) L.k++;
+            else { L.st = S_EGP; L.nbits = 0; L.ret = R_MAG; }
+        } else {
+            // magnitude k+1 complete: sign bypass (src/mc_codec.c:205,369)
+            const uint32_t half = L.range >> 1;
+            const uint32_t neg = L.code >= half ? 1u : 0u;
+            L.code -= neg ? half : 0u;
+            L.range = half;
+            renorm(L);
+            const uint32_t m = L.k + 1;
+            put_entry(L, P, (sc & 0xFFFu) | ((neg ? 0u - m : m) << 16));
+            if (L.st != S_DONE) { L.p++; advance(L); }
+        }
+    } else if (st == F_HDR) {                        // flag0, flag1, dc bits 7..0
+        L.hdr = (L.hdr << 1) | bit;
+        if (++L.k == 10) { L.st = F_EOBP; L.k = 0; L.lbase = kCtxEob; }
+    } else {                                          // F_EOBP (src/mc_codec.c:321-327)
+        if (!(bit && ++L.k < 13)) {
+            if (L.k < 2) { L.eob = L.k; L.p = 0; L.hist = 0; advance(L); }
+            else { L.st = S_EOBS; L.k = L.k - 1; }
+        }
+    }
+}
+
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
-    __shared__ uint16_t s_scan[kN3];
-    __shared__ uint32_t s_ctx[WARPS][kNumCtx][32];
-    for (int i = threadIdx.x; i < kN3; i += blockDim.x) s_scan[i] = P.scan[i];
+    __shared__ uint32_t s_scan[kN3];   // raster idx | (24 + 4*band) << 12
+    __shared__ uint16_t s_ctx[WARPS][kNumCtx][32];
+    for (int i = threadIdx.x; i < kN3; i += blockDim.x) {
+        const uint32_t v = P.scan[i];
+        s_scan[i] = (v & 0xFFFu) | ((uint32_t)kCtxSig + 4u * (v >> 12)) << 12;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t *ctx = &s_ctx[warp][0][lane];
+    uint16_t *ctx = &s_ctx[warp][0][lane];
 
     const int stride = gridDim.x * blockDim.x;
     int next = blockIdx.x * blockDim.x + threadIdx.x;
     LaneState L;
-    L.state = S_IDLE;
+    NextItem N;
+    L.st = S_IDLE;
     L.item = -1;
-    auto claim = [&]() -> bool {
-        while (next < P.n) {
-            int slot = P.order ? (int)P.order[next] : next;
-            next += stride;
-            lane_begin(L, P, ctx, slot);
-            if (L.state != S_DONE) return true;
-            lane_finish(L, P);
-        }
-        L.state = S_IDLE;
-        return false;
-    };
-    claim();
+    prefetch_item(N, P, next);
+    next += stride;
+    // start the first block (skipping absent ones)
+    while (N.slot >= 0) {
+        lane_begin(L, P, ctx, N);
+        prefetch_item(N, P, next);
+        next += stride;
+        if (L.st != S_DONE) break;
+        lane_finish(L, P);
+        L.st = S_IDLE;
+    }
 
-    // Every iteration decodes at most one bin per lane; a bounded number of
-    // iterations per block follows from the Exp-Golomb cap and the finite
-    // scan, so the loop always terminates.
-    while (__any_sync(0xFFFFFFFFu, L.state != S_IDLE)) {
-        if (L.state == S_IDLE) continue;
-        const uint32_t st = L.state;
-        uint32_t bit;
-        if (st < S_EOBS) {
-            // ---- context-coded bin (src/mc_codec.c:198-204)
-            uint32_t cidx;
-            if (st == S_SIG) {
-                uint32_t sc = s_scan[L.p];
-                uint32_t dens = min(__popc(L.hist & 0xFFFFu), 3);
-                cidx = kCtxSig + (sc >> 12) * 4 + dens;
-            } else {
-                // FLAG 0, DC 2, EOB 10, MAG 56 (+k)
-                const uint32_t base = st == S_FLAG ? kCtxFlag : st == S_DC ? kCtxDc : st == S_EOBP ? kCtxEob : kCtxMag;
-                cidx = base + L.k;
-            }
-            uint32_t p0 = ctx[cidx * 32];
-            uint32_t r0 = (L.range >> 12) * p0;
-            if (L.code < r0) {
-                L.range = r0; bit = 0; p0 += (4096u - p0) >> 4;
-            } else {
-                L.code -= r0; L.range -= r0; bit = 1; p0 -= p0 >> 4;
-            }
-            ctx[cidx * 32] = p0;
-        } else {
-            // ---- bypass bits, k at once (src/mc_codec.c:205,216-226)
-            uint32_t nb = (st == S_EOBS) ? L.k : (st == S_EGS ? min(L.rem, 16u) : 1u);
-            L.range >>= nb;
-            uint32_t q;
-            if (nb == 1) q = L.code >= L.range ? 1u : 0u;
-            else { q = L.code / L.range; uint32_t mx = (1u << nb) - 1u; q = q > mx ? mx : q; }
-            L.code -= q * L.range;
-            bit = q;
+    // Inner loop: only the fast step, for as long as every live lane is in a
+    // fast state (idle lanes sit it out). Outer loop: the slow bypass steps and
+    // block switches, entered when some lane needs one. Every block ends after
+    // a bounded number of bins (finite scan, capped Exp-Golomb prefixes), so
+    // both loops terminate.
+    for (;;) {
+        while (__all_sync(0xFFFFFFFFu, L.st <= F_MAG || L.st == S_IDLE) &&
+               __any_sync(0xFFFFFFFFu, L.st != S_IDLE)) {
+            if (L.st <= F_MAG) fast_step(L, P, ctx, s_scan);
         }
-        while (L.range < (1u << 24)) { L.code = (L.code << 8) | fetch(L); L.range <<= 8; }
-
-        switch (st) {
-        case S_FLAG:
-            L.flags |= bit << L.k;
-            if (++L.k == 2) { L.state = S_DC; L.k = 0; }
-            break;
-        case S_DC:
-            L.dc = (L.dc << 1) | bit;
-            if (++L.k == 8) { L.state = S_EOBP; L.k = 0; }
-            break;
-        case S_EOBP:   // bit length of eob, 13 context bins at most (src/mc_codec.c:321-327)
-            if (bit && ++L.k < 13) break;
-            if (L.k == 0) { L.eob = 0; L.p = 0; goto_position(L); }
-            else if (L.k == 1) { L.eob = 1; L.p = 0; L.hist = 0; goto_position(L); }
-            else { L.state = S_EOBS; L.k = L.k - 1; }
-            break;
-        case S_EOBS:
-            L.eob = (1u << L.k) | bit;
-            if (L.eob > (uint32_t)kN3) L.eob = kN3;
-            L.p = 0; L.hist = 0;
-            goto_position(L);
-            break;
-        case S_SIG:
-            L.hist = (L.hist << 1) | bit;
-            if (bit) { L.state = S_MAG; L.k = 0; }
-            else { L.p++; goto_position(L); }
-            break;
-        case S_MAG:    // 12 adaptive unary rungs (src/mc_codec.c:268-275)
-            if (!bit) { L.mag = L.k + 1; L.state = S_SIGN; }
-            else if (L.k < 11) L.k++;
-            else { L.state = S_EGP; L.nbits = 0; L.ret = R_MAG; }
-            break;
-        case S_SIGN: {
-            uint32_t sc = s_scan[L.p];
-            uint32_t idx = sc & 0xFFFu;
-            int32_t lv = bit ? -(int32_t)L.mag : (int32_t)L.mag;
-            put_entry(L, P, idx | ((uint32_t)(uint16_t)(int16_t)lv << 16));
-            if (L.state == S_DONE) break;
-            L.nnz++;
-            L.ez = max(L.ez, (int)(idx >> 8));
-            L.ey = max(L.ey, (int)((idx >> 4) & 15));
-            L.ex = max(L.ex, (int)(idx & 15));
-            L.p++;
-            goto_position(L);
-            break;
-        }
-        case S_EGP:    // Exp-Golomb prefix: count one-bits (src/mc_codec.c:234-238)
-            if (bit) {
-                if (++L.nbits >= (uint32_t)kEgCap) { L.bad = 1; L.state = S_DONE; }
-            } else if (L.nbits == 0) {
-                eg_return(L, P, s_scan, 0);
-            } else {
-                L.state = S_EGS; L.rem = L.nbits; L.acc = 0;
-            }
-            break;
-        case S_EGS: {
-            uint32_t nb = min(L.rem, 16u);
-            L.acc = (L.acc << nb) | bit;
-            L.rem -= nb;
-            if (L.rem == 0) eg_return(L, P, s_scan, ((1u << (L.nbits & 31)) | L.acc) - 1u);
-            break;
-        }
-        case S_CSIGN:
-            L.cneg = bit;
-            L.state = S_EGP; L.nbits = 0; L.ret = R_CMAG;
-            break;
-        default:
-            break;
-        }
-        if (L.state == S_DONE) {
+        if (!__any_sync(0xFFFFFFFFu, L.st != S_IDLE)) break;
+        if (L.st <= F_MAG) fast_step(L, P, ctx, s_scan);
+        else if (L.st < S_DONE) slow_step(L, P, s_scan);
+        if (L.st == S_DONE) {
             lane_finish(L, P);
-            claim();
+            L.st = S_IDLE;
+            while (N.slot >= 0) {
+                lane_begin(L, P, ctx, N);
+                prefetch_item(N, P, next);
+                next += stride;
+                if (L.st != S_DONE) break;
+                lane_finish(L, P);
+                L.st = S_IDLE;
+            }
         }
     }
 }
@@ -304,135 +421,289 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 
+// Packed pairs: sm_100 executes two IEEE single-precision round-to-nearest
+// adds or multiplies per instruction (add/sub/mul.rn.f32x2), each lane of the
+// pair rounding exactly like its scalar __fadd_rn / __fmul_rn. One caution,
+// measured with ptxas 12.9 on sm_100a: a packed multiply whose result feeds a
+// packed add is contracted into a single-rounding packed FMA despite the .rn
+// qualifiers (even inside one asm statement, and also when the product is
+// written as fma with a -0 addend). The multiply-accumulates below therefore
+// pair a packed multiply with scalar __fadd_rn adds, a combination that keeps
+// both roundings; packed adds are used only on sums.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+// acc + w*v per lane with two roundings (see above)
+__device__ __forceinline__ float2 madd2(float2 acc, float2 w, float2 v) {
+    const float2 p = mul2(w, v);
+    return make_float2(__fadd_rn(acc.x, p.x), __fadd_rn(acc.y, p.y));
+}
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+// 4 adjacent lines x 2 outputs (m, m+1): even-k and odd-k halves, each a
+// sequential sum over ascending k (src/mc_codec_float.h:102-104). in[k*ks]
+// holds the 4 lines' k-th inputs, W[k*16 + m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}.
+struct Acc4 { float2 e0a, e0b, e1a, e1b, o0a, o0b, o1a, o1b; };
+__device__ __forceinline__ Acc4 lines4(const float4 *in, int ks, int K, const float4 *W, int mh) {
+    Acc4 a;
+    const float2 z = make_float2(0.f, 0.f);
+    a.e0a = a.e0b = a.e1a = a.e1b = a.o0a = a.o0b = a.o1a = a.o1b = z;
+    for (int k = 0; k < K; k += 2) {
+        const float4 v = in[k * ks], w = W[k * 8 + mh];
+        const float2 w0 = lo2(w), w1 = hi2(w);
+        a.e0a = madd2(a.e0a, w0, lo2(v)); a.e0b = madd2(a.e0b, w0, hi2(v));
+        a.e1a = madd2(a.e1a, w1, lo2(v)); a.e1b = madd2(a.e1b, w1, hi2(v));
+        if (k + 1 < K) {
+            const float4 u = in[(k + 1) * ks], x = W[(k + 1) * 8 + mh];
+            const float2 x0 = lo2(x), x1 = hi2(x);
+            a.o0a = madd2(a.o0a, x0, lo2(u)); a.o0b = madd2(a.o0b, x0, hi2(u));
+            a.o1a = madd2(a.o1a, x1, lo2(u)); a.o1b = madd2(a.o1b, x1, hi2(u));
+        }
+    }
+    return a;
+}
+
 __device__ __forceinline__ uint32_t entry_at(const RecParams &P, uint64_t base, uint32_t cap, uint32_t ovf, uint32_t j) {
     if (j < cap) return P.arena[base + j];
     return ovf == 0xFFFFFFFFu ? 0u : P.pool[ovf + (j - cap)];
 }
 
-__device__ __forceinline__ uint8_t to_u8(float v, int dc) {
-    long long r = __float2ll_rn(v);          // lrintf: round half to even
-    int s = (int)(uint32_t)(unsigned long long)r + dc;
-    return (uint8_t)(s < 0 ? 0 : s > 255 ? 255 : s);
+// (int)lrintf(v) + dc clamped to u8 (src/mc_codec.c:766-769). Adding 1.5*2^23
+// rounds to an integer half-to-even for |v| < 2^22, which is exactly lrintf;
+// larger values (only from corrupt streams) take the 64-bit conversion.
+__device__ __forceinline__ uint32_t to_u8(float v, int dc) {
+    int r;
+    if (fabsf(v) < 4194304.0f) {
+        r = __float_as_int(fadd(v, 12582912.0f)) - 0x4B400000;
+    } else {
+        r = (int)(uint32_t)(unsigned long long)__float2ll_rn(v);
+    }
+    const int s = r + dc;
+    return (uint32_t)(s < 0 ? 0 : s > 255 ? 255 : s);
+}
+// four voxels (x, x+1 | x+2, x+3) -> little-endian u8x4
+__device__ __forceinline__ uint32_t pack4(float2 a, float2 b, int dc) {
+    return to_u8(a.x, dc) | (to_u8(a.y, dc) << 8) | (to_u8(b.x, dc) << 16) | (to_u8(b.y, dc) << 24);
 }
 
-// one transform line: e/o halves for outputs (m, m+1) over k < K,
-// sequential in k (src/mc_codec_float.h:102-104)
-__device__ __forceinline__ void line_pair(const float *in, int si, int K, int m,
-                                          float &e0, float &e1, float &o0, float &o1) {
-    e0 = e1 = o0 = o1 = 0.0f;
-    for (int k = 0; k < K; k += 2) {
-        float v = in[k * si];
-        e0 = fadd(e0, fmul(c_cos[k][m], v));
-        e1 = fadd(e1, fmul(c_cos[k][m + 1], v));
+// Shared-memory row strides (floats / bytes), padded so that the lanes of a
+// warp that write the four outputs (m, m+1, 15-m, 14-m) of a line hit four
+// different banks.
+constexpr int kRowF = 20;            // A and B rows of 16 floats
+constexpr int kPlaneB = 16 * kRowF;  // one cz plane of B
+constexpr int kStageZ = 272;         // stage: one z slice of 16 rows of 16 bytes
+constexpr int kStageBytes = 16 * kStageZ;
+
+// Reconstruct one block into a stage (z slices of kStageZ bytes). Thread t owns the
+// output pair (m, m+1) = 2*(t&3) of every line it touches; its cosine weights
+// come from the shared table W.
+__device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, float *sA, float *sB,
+                                                  uint8_t *stage, const float4 *W) {
+    const int tid = threadIdx.x;
+    const int m = (tid & 3) * 2;
+    const DecItem it = P.items[item];
+    const EntHdr h = P.hdr[item];
+    const uint64_t base = P.base[item];
+    const uint32_t cap = entry_cap(it.len);
+    // the header comes from k_entropy; the guards keep every index below
+    // inside shared memory whatever its contents
+    const bool sane = h.nnz <= kN3 && h.ncorr <= kN3;
+    const int dc = it.len && sane ? h.dc : 0;
+    const int nnz = it.len && sane ? h.nnz : 0;
+    const int ncorr = it.len && sane ? h.ncorr : 0;
+
+    if (nnz == 0) {
+        // constant block (src/mc_codec.c:757-759) or absent block (zeros)
+        const uint32_t w = (uint32_t)dc * 0x01010101u;
+        const uint4 v = make_uint4(w, w, w, w);
+        for (int i = tid; i < kStageBytes / 16; i += 128) reinterpret_cast<uint4 *>(stage)[i] = v;
+    } else {
+        // extents of the coefficient box: largest cz, cy, cx of any entry
+        // (src/mc_codec.c:371-372)
+        __shared__ int s_ext[3];
+        if (tid < 3) s_ext[tid] = 0;
+        __syncthreads();
+        int mz = 0, my = 0, mx = 0;
+        for (int j = tid; j < nnz; j += 128) {
+            const uint32_t e = entry_at(P, base, cap, h.ovf, j);
+            mz = max(mz, (int)((e >> 8) & 15));
+            my = max(my, (int)((e >> 4) & 15));
+            mx = max(mx, (int)(e & 15));
+        }
+        atomicMax(&s_ext[0], mz);
+        atomicMax(&s_ext[1], my);
+        atomicMax(&s_ext[2], mx);
+        __syncthreads();
+        const int E = s_ext[0] + 1, Y = s_ext[1] + 1, X = s_ext[2] + 1;
+        const QTab &qt = P.qtab[it.qslot];
+        for (int i = tid; i < E * Y * X; i += 128) sB[i] = 0.0f;
+        __syncthreads();
+        // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
+        for (int j = tid; j < nnz; j += 128) {
+            const uint32_t e = entry_at(P, base, cap, h.ovf, j);
+            const int idx = e & 0xFFF;
+            const int lv = (int16_t)(e >> 16);
+            if (!lv) continue;
+            const int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;
+            if (cz >= E || cy >= Y || cx >= X) continue;
+            const int f = cz + cy + cx;
+            const float a = (float)(lv < 0 ? -lv : lv);
+            const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
+            sB[(cz * Y + cy) * X + cx] = lv < 0 ? -r : r;
+        }
+        __syncthreads();
+        // pass 1: lines along x (cz,cy), box -> A[cz][cy][x]; the output pair
+        // (m, m+1) of one line accumulates as one packed pair
+        const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
+        for (int t = tid; t < E * Y * 4; t += 128) {
+            const int line = t >> 2;
+            const float *in = sB + line * X;
+            float2 e = make_float2(0.f, 0.f), o = e;
+            for (int k = 0; k < X; k += 2) {
+                const float v = in[k];
+                const float4 w = W[k * 8 + mh];
+                e = madd2(e, make_float2(w.x, w.z), make_float2(v, v));
+                if (k + 1 < X) {
+                    const float u = in[k + 1];
+                    const float4 x = W[(k + 1) * 8 + mh];
+                    o = madd2(o, make_float2(x.x, x.z), make_float2(u, u));
+                }
+            }
+            const float2 sum = add2(e, o), dif = sub2(e, o);
+            float *out = sA + line * kRowF;
+            out[m] = sum.x;
+            out[m + 1] = sum.y;
+            out[15 - m] = dif.x;
+            out[14 - m] = dif.y;
+        }
+        __syncthreads();
+        // pass 2: lines along y for 4 adjacent x at once, A[cz][k][x..x+3] -> B[cz][y][x..x+3]
+        for (int t = tid; t < E * 16; t += 128) {
+            const int xg = (t >> 2) & 3, cz = t >> 4;
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sA + cz * Y * kRowF + xg * 4), kRowF / 4, Y,
+                                  W, mh);
+            float4 *o = reinterpret_cast<float4 *>(sB + cz * kPlaneB + xg * 4);
+            constexpr int R = kRowF / 4;
+            const float2 p0 = add2(a.e0a, a.o0a), p1 = add2(a.e0b, a.o0b);
+            const float2 q0 = add2(a.e1a, a.o1a), q1 = add2(a.e1b, a.o1b);
+            const float2 r0 = sub2(a.e0a, a.o0a), r1 = sub2(a.e0b, a.o0b);
+            const float2 s0 = sub2(a.e1a, a.o1a), s1 = sub2(a.e1b, a.o1b);
+            o[m * R] = make_float4(p0.x, p0.y, p1.x, p1.y);
+            o[(m + 1) * R] = make_float4(q0.x, q0.y, q1.x, q1.y);
+            o[(15 - m) * R] = make_float4(r0.x, r0.y, r1.x, r1.y);
+            o[(14 - m) * R] = make_float4(s0.x, s0.y, s1.x, s1.y);
+        }
+        __syncthreads();
+        // pass 3: lines along z for 4 adjacent x, B[k][y][x..x+3] -> voxels
+        for (int t = tid; t < 256; t += 128) {
+            const int xg = (t >> 2) & 3, y = t >> 4;
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + y * kRowF + xg * 4), kPlaneB / 4, E, W, mh);
+            uint32_t *row = reinterpret_cast<uint32_t *>(stage + y * 16 + xg * 4);
+            constexpr int Z = kStageZ / 4;
+            row[m * Z] = pack4(add2(a.e0a, a.o0a), add2(a.e0b, a.o0b), dc);
+            row[(m + 1) * Z] = pack4(add2(a.e1a, a.o1a), add2(a.e1b, a.o1b), dc);
+            row[(15 - m) * Z] = pack4(sub2(a.e0a, a.o0a), sub2(a.e0b, a.o0b), dc);
+            row[(14 - m) * Z] = pack4(sub2(a.e1a, a.o1a), sub2(a.e1b, a.o1b), dc);
+        }
     }
-    for (int k = 1; k < K; k += 2) {
-        float v = in[k * si];
-        o0 = fadd(o0, fmul(c_cos[k][m], v));
-        o1 = fadd(o1, fmul(c_cos[k][m + 1], v));
+    __syncthreads();
+    if (ncorr && tid == 0) {
+        // corrections in stream order: a position may repeat, each
+        // application clamps (src/mc_codec.c:775-781)
+        for (int c = 0; c < ncorr; ++c) {
+            const uint32_t pos = entry_at(P, base, cap, h.ovf, nnz + 2 * c);
+            const uint32_t d = entry_at(P, base, cap, h.ovf, nnz + 2 * c + 1);
+            if (pos >= (uint32_t)kN3) break;
+            uint8_t &vox = stage[(pos >> 8) * kStageZ + (pos & 255)];
+            const int v = (int)((uint32_t)vox + d);
+            vox = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        }
     }
+    __syncthreads();
+}
+
+// Clipped store of one staged block: one 16-voxel row per thread step.
+__device__ __forceinline__ void store_block(const DecItem &it, const uint8_t *stage) {
+    const int z0 = it.clip_lo >> 8, y0 = (it.clip_lo >> 4) & 15, x0 = it.clip_lo & 15;
+    const int z1 = it.clip_hi >> 8, y1 = (it.clip_hi >> 4) & 15, x1 = it.clip_hi & 15;
+    const int ny = y1 - y0 + 1, nrows = (z1 - z0 + 1) * ny;
+    uint8_t *dst = reinterpret_cast<uint8_t *>(it.dst);
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+        const int z = z0 + r / ny, y = y0 + r % ny;
+        uint8_t *row = dst + z * it.sz + y * it.sy;
+        const uint8_t *srow = stage + z * kStageZ + y * 16;
+        if (x0 == 0 && x1 == 15 && ((uintptr_t)row & 15) == 0) {
+            *reinterpret_cast<uint4 *>(row) = *reinterpret_cast<const uint4 *>(srow);
+        } else {
+            for (int x = x0; x <= x1; ++x) row[x] = srow[x];
+        }
+    }
+}
+
+// Two blocks that sit side by side in x in the same output: one 32-byte
+// row per step, so every DRAM sector is written whole (16-byte halves of a
+// sector written apart cost a read-modify-write).
+__device__ __forceinline__ bool pairable(const DecItem &a, const DecItem &b) {
+    return a.clip_lo == kClipFullLo && a.clip_hi == kClipFullHi && b.clip_lo == kClipFullLo &&
+           b.clip_hi == kClipFullHi && b.dst == a.dst + 16 && a.sz == b.sz && a.sy == b.sy && (a.dst & 31) == 0 &&
+           (a.sy & 31) == 0 && (a.sz & 31) == 0;
 }
 
 __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
-    __shared__ __align__(16) float sA[kN3];
-    __shared__ __align__(16) float sB[kN3];
-    uint8_t *stage = reinterpret_cast<uint8_t *>(sA);
+    // sA: pass-1 output, then the second block's stage; sB: coefficient box,
+    // then pass-2 output; sStage0: the first block's stage
+    __shared__ __align__(16) float sA[16 * 16 * kRowF];
+    __shared__ __align__(16) float sB[16 * kPlaneB];
+    __shared__ __align__(16) uint8_t sStage0[kStageBytes];
+    __shared__ __align__(16) float4 sW[16 * 8];   // [k][m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}
+    uint8_t *const sStage1 = reinterpret_cast<uint8_t *>(sA);
+    for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
+        const int k = i >> 3, mm = (i & 7) * 2;
+        sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
+    }
+    __syncthreads();
     const int tid = threadIdx.x;
-
-    for (int item = blockIdx.x; item < P.n; item += gridDim.x) {
-        const DecItem it = P.items[item];
-        const EntHdr h = P.hdr[item];
-        const uint64_t base = P.base[item];
-        const uint32_t cap = entry_cap(it.len);
-        // the header comes from k_entropy; the guards keep every index below
-        // inside shared memory whatever its contents
-        const bool sane = h.ez <= 15 && h.ey <= 15 && h.ex <= 15 && h.nnz <= kN3 && h.ncorr <= kN3 &&
-                          (h.nnz == 0 || (h.ez >= 0 && h.ey >= 0 && h.ex >= 0));
-        const int dc = it.len && sane ? h.dc : 0;
-        const int nnz = it.len && sane ? h.nnz : 0;
-        const int ncorr = it.len && sane ? h.ncorr : 0;
-
-        if (nnz == 0) {
-            // constant block (src/mc_codec.c:757-759) or absent block (zeros)
-            uint32_t w = (uint32_t)dc * 0x01010101u;
-            uint4 v = make_uint4(w, w, w, w);
-            for (int i = tid; i < kN3 / 16; i += 128) reinterpret_cast<uint4 *>(stage)[i] = v;
-        } else {
-            const int E = h.ez + 1, Y = h.ey + 1, X = h.ex + 1;
-            const QTab &qt = P.qtab[it.qslot];
-            for (int i = tid; i < E * Y * X; i += 128) sB[i] = 0.0f;
-            __syncthreads();
-            // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
-            for (int j = tid; j < nnz; j += 128) {
-                uint32_t e = entry_at(P, base, cap, h.ovf, j);
-                int idx = e & 0xFFF;
-                int lv = (int16_t)(e >> 16);
-                if (!lv) continue;
-                int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;
-                if (cz >= E || cy >= Y || cx >= X) continue;
-                int f = cz + cy + cx;
-                float a = (float)(lv < 0 ? -lv : lv);
-                float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
-                sB[(cz * Y + cy) * X + cx] = lv < 0 ? -r : r;
-            }
-            __syncthreads();
-            // pass 1: lines along x, box -> A[cz][cy][x]
-            for (int t = tid; t < E * Y * 4; t += 128) {
-                int line = t >> 2, m = (t & 3) * 2;
-                float e0, e1, o0, o1;
-                line_pair(sB + line * X, 1, X, m, e0, e1, o0, o1);
-                float *o = sA + line * 16;
-                o[m] = fadd(e0, o0); o[m + 1] = fadd(e1, o1);
-                o[15 - m] = fsub(e0, o0); o[14 - m] = fsub(e1, o1);
-            }
-            __syncthreads();
-            // pass 2: lines along y, A[cz][k][x] -> B[cz][y][x]
-            for (int t = tid; t < E * 64; t += 128) {
-                int m = (t & 3) * 2, x = (t >> 2) & 15, cz = t >> 6;
-                float e0, e1, o0, o1;
-                line_pair(sA + cz * Y * 16 + x, 16, Y, m, e0, e1, o0, o1);
-                float *o = sB + cz * 256 + x;
-                o[m * 16] = fadd(e0, o0); o[(m + 1) * 16] = fadd(e1, o1);
-                o[(15 - m) * 16] = fsub(e0, o0); o[(14 - m) * 16] = fsub(e1, o1);
-            }
-            __syncthreads();
-            // pass 3: lines along z, B[k][y][x] -> voxels, lrint + dc, clamp
-            for (int t = tid; t < 256 * 4; t += 128) {
-                int m = (t & 3) * 2, line = t >> 2;
-                float e0, e1, o0, o1;
-                line_pair(sB + line, 256, E, m, e0, e1, o0, o1);
-                stage[m * 256 + line] = to_u8(fadd(e0, o0), dc);
-                stage[(m + 1) * 256 + line] = to_u8(fadd(e1, o1), dc);
-                stage[(15 - m) * 256 + line] = to_u8(fsub(e0, o0), dc);
-                stage[(14 - m) * 256 + line] = to_u8(fsub(e1, o1), dc);
-            }
-        }
-        __syncthreads();
-        if (ncorr && tid == 0) {
-            // corrections in stream order: a position may repeat, each
-            // application clamps (src/mc_codec.c:775-781)
-            for (int c = 0; c < ncorr; ++c) {
-                uint32_t pos = entry_at(P, base, cap, h.ovf, nnz + 2 * c);
-                uint32_t d = entry_at(P, base, cap, h.ovf, nnz + 2 * c + 1);
-                if (pos >= (uint32_t)kN3) break;
-                int v = (int)((uint32_t)stage[pos] + d);
-                stage[pos] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
-            }
-        }
-        __syncthreads();
-        // clipped store: one 16-voxel row per thread step
-        const int z0 = it.clip_lo >> 8, y0 = (it.clip_lo >> 4) & 15, x0 = it.clip_lo & 15;
-        const int z1 = it.clip_hi >> 8, y1 = (it.clip_hi >> 4) & 15, x1 = it.clip_hi & 15;
-        const int ny = y1 - y0 + 1, nrows = (z1 - z0 + 1) * ny;
-        uint8_t *dst = reinterpret_cast<uint8_t *>(it.dst);
-        for (int r = tid; r < nrows; r += 128) {
-            int z = z0 + r / ny, y = y0 + r % ny;
-            uint8_t *row = dst + z * it.sz + y * it.sy;
-            const uint8_t *srow = stage + z * 256 + y * 16;
-            if (x0 == 0 && x1 == 15 && ((uintptr_t)row & 15) == 0) {
-                *reinterpret_cast<uint4 *>(row) = *reinterpret_cast<const uint4 *>(srow);
+    const int npairs = (P.n + 1) / 2;
+    for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
+        const int i0 = 2 * pr, i1 = 2 * pr + 1;
+        reconstruct_block(P, i0, sA, sB, sStage0, sW);
+        const DecItem a = P.items[i0];
+        if (i1 < P.n) {
+            reconstruct_block(P, i1, sA, sB, sStage1, sW);
+            const DecItem b = P.items[i1];
+            if (pairable(a, b)) {
+                uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
+                for (int r = tid; r < 256; r += 128) {
+                    const int z = r >> 4, y = r & 15;
+                    uint4 *row = reinterpret_cast<uint4 *>(dst + z * a.sz + y * a.sy);
+                    row[0] = *reinterpret_cast<const uint4 *>(sStage0 + z * kStageZ + y * 16);
+                    row[1] = *reinterpret_cast<const uint4 *>(sStage1 + z * kStageZ + y * 16);
+                }
             } else {
-                for (int x = x0; x <= x1; ++x) row[x] = srow[x];
+                store_block(a, sStage0);
+                store_block(b, sStage1);
             }
+        } else {
+            store_block(a, sStage0);
         }
         __syncthreads();
     }
@@ -467,8 +738,8 @@ cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_
 
 cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStream_t s) {
     if (p.n <= 0) return cudaSuccess;
-    int blocks = p.n;
-    int cap = num_sms() * (cfg.rec_ctas_per_sm > 0 ? cfg.rec_ctas_per_sm : 6);
+    int blocks = (p.n + 1) / 2;   // one CTA step per pair of blocks
+    int cap = num_sms() * (cfg.rec_ctas_per_sm > 0 ? cfg.rec_ctas_per_sm : 5);
     if (blocks > cap) blocks = cap;
     k_reconstruct<<<blocks, 128, 0, s>>>(p);
     return cudaGetLastError();

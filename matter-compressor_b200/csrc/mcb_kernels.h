@@ -9,8 +9,8 @@ namespace mcb {
 
 // Launch shape knobs, picked per quality by the autotuner.
 struct LaunchCfg {
-    int ent_ctas_per_sm = 8;   // entropy stage: CTAs of 4 warps per SM
-    int rec_ctas_per_sm = 6;   // reconstruction stage: CTAs of 128 threads per SM
+    int ent_ctas_per_sm = 6;   // entropy stage: CTAs of 4 warps per SM (<= 6: 75 regs, 34 KB smem)
+    int rec_ctas_per_sm = 5;   // reconstruction stage: CTAs of 128 threads per SM (<= 5: 40 KB smem)
 };
 
 struct EntParams {

@@ -173,13 +173,31 @@ bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t 
         B.subs.emplace_back(i0, i1);
         i0 = i1;
     }
-    if (!B.items.ensure(sizeof(DecItem) * (size_t)n) || !B.base.ensure(sizeof(uint64_t) * (size_t)n) ||
+    // entropy-stage order within each sub-batch: longest payload first
+    // (counting sort by length), so the lanes of a warp decode blocks of
+    // similar size and the per-lane totals balance (longest-processing-time-first)
+    std::vector<uint32_t> order((size_t)n);
+    {
+        std::vector<uint32_t> cnt(65536);
+        for (auto &r : B.subs) {
+            std::fill(cnt.begin(), cnt.end(), 0u);
+            auto key = [&](int i) { return 65535u - std::min<uint32_t>(h_items[i].len, 65535u); };
+            for (int i = r.first; i < r.second; ++i) cnt[key(i)]++;
+            uint32_t acc = 0;
+            for (auto &c : cnt) { uint32_t t = c; c = acc; acc += t; }
+            for (int i = r.first; i < r.second; ++i) order[r.first + cnt[key(i)]++] = (uint32_t)(i - r.first);
+        }
+    }
+    if (!B.order.ensure(sizeof(uint32_t) * (size_t)n) || !B.items.ensure(sizeof(DecItem) * (size_t)n) ||
+        !B.base.ensure(sizeof(uint64_t) * (size_t)n) ||
         !B.hdr.ensure(sizeof(EntHdr) * (size_t)n) || !B.arena.ensure(sizeof(uint32_t) * max_acc) ||
         !B.pool.ensure(sizeof(uint32_t) * kPoolEntries) || !B.status.ensure(16))
         return false;
     // synchronous copies: the host arrays may be pageable and short-lived
     return cuda_ok(cudaMemcpyAsync(B.items.p, h_items, sizeof(DecItem) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D items") &&
+           cuda_ok(cudaMemcpyAsync(B.order.p, order.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s),
+                   "H2D order") &&
            cuda_ok(cudaMemcpyAsync(B.base.p, hb.data(), sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D base") &&
            cuda_ok(cudaStreamSynchronize(s), "sync");
@@ -193,7 +211,7 @@ bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
         const int i0 = r.first, m = r.second - r.first;
         EntParams ep;
         ep.items = B.items.as<DecItem>() + i0;
-        ep.order = nullptr;
+        ep.order = B.order.as<uint32_t>() + i0;
         ep.n = m;
         ep.base = B.base.as<uint64_t>() + i0;
         ep.arena = B.arena.as<uint32_t>();

@@ -62,7 +62,7 @@ int qslot(float q);
 // host item array and uploads items and offsets; decode_enqueue launches the
 // two stages (capturable into a CUDA graph).
 struct DecodeBatch {
-    DevBuf items, base, hdr, arena, pool, status;
+    DevBuf items, order, base, hdr, arena, pool, status;
     int n = 0;
     std::vector<std::pair<int, int>> subs;   // [i0, i1) ranges that fit the arena
 };
