@@ -1,0 +1,357 @@
+"""Batched chunk decode benchmark: decoded GB/s per B200 at q=6.
+
+Workload (per rank): 64 synthetic 256^3 u8 chunks (1 GiB raw; seeds
+rank*64 .. rank*64+63, air fraction 30-60 %), encoded at q=6 into an archive
+whose bytes are resident in HBM; one step decodes every block of every chunk
+through a graph-captured decode plan (entropy stage + reconstruction stage).
+
+  value     decoded bytes of all ranks / max-over-ranks step time (CUDA events
+            on the launching stream; the L2 is flushed by a 256 MiB write
+            between steps, outside the timed events)
+  e2e       the same metric through mc_b200_decode_chunk_blobs with HOST
+            buffers: compressed blobs host->device and voxels device->host
+            inside every step (pinned host memory)
+  roofline  the dominant kernel (entropy stage) timed alone with CUDA events,
+            decoded bytes per launch / its time, against the measured HBM peak
+  cpu_baseline  the reference's own decode (its sources built with its default
+            optimisation flags, oracle/_ref/libmcref_fast.so) on this host's
+            cores, mc_archive_decode_chunk(nthreads=0), rank 0 at N=1 only
+
+`--impl reference` runs only the reference's CPU decode of the same workload
+(rank 0; other ranks exit) and prints the same JSON line with "impl": "reference".
+Multi-GPU: python -m torch.distributed.run --nproc-per-node N bench.py --gpus N
+(weak scaling: every rank decodes its own 64 chunks; no data-path collective).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "matter-compressor_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+from shard import Dist, chunk_seeds, air_fraction  # noqa: E402
+
+CHUNK = 256 ** 3
+METRIC = "decoded GB/s per B200 at q=6 (bit-exact); p50/p99 block-request latency"
+HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes per decoded chunk of the entropy stage, measured with ncu on an
+# 8-chunk case and scaled per chunk (profiles/k_entropy_decode_q6.md).
+ENTROPY_DRAM_BYTES_PER_CHUNK = None
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--chunks", type=int, default=64)
+    p.add_argument("--q", type=float, default=6.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_volumes(seeds, device):
+    import volumes
+    out = torch.empty((len(seeds), 256, 256, 256), dtype=torch.uint8, device=device)
+    for i, s in enumerate(seeds):
+        out[i] = volumes.region(s, (0, 0, 256 * i), (256, 256, 256), air_fraction(i), device=device)
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of the GPU's SM clock and throttle reasons while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc, self.path = None, None
+
+    def start(self):
+        try:
+            uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+            ident = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            ident = "0"
+        self.path = tempfile.mktemp(suffix=".csv")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ident, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms",
+                 "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.remove(self.path)
+        if not rows:
+            return None
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[0]) for r in rows if num(r[0]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[4:8]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][1]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def blobs_of(path, offs):
+    """Chunk blobs of an archive file (header, fmap, bitmap, lengths, payloads)."""
+    data = np.fromfile(path, np.uint8)
+    out = []
+    for co in offs:
+        fml = int(data[co + 12]) | (int(data[co + 13]) << 8)
+        bm = data[co + 14 + fml:co + 14 + fml + 512]
+        npres = int(np.unpackbits(bm).sum())
+        lens = data[co + 14 + fml + 512:co + 14 + fml + 512 + 2 * npres].view(np.uint16).astype(np.int64)
+        n = 14 + fml + 512 + 2 * npres + int(lens.sum())
+        out.append(data[co:co + n])
+    return out
+
+
+# ------------------------------------------------------------------ reference CPU decode
+def reference_decode(path, nchunks, q, steps, warmup, min_seconds=0.0):
+    """The reference's own mc_archive_decode_chunk(nthreads=0) over the archive."""
+    from mcb200 import McLib
+    from oracle import REF_FAST_LIB
+    ref = McLib(REF_FAST_LIB, b200=False)
+    ref.L.mc_codec_init()
+    a = ref.open(path, 256 * nchunks, 256, 256, q)
+    offs = [a.chunk_offset(0, 0, 0, c) for c in range(nchunks)]
+    out = np.empty(CHUNK, np.uint8)
+    for _ in range(warmup):
+        a.decode_chunk(offs[0], out, 0)
+    times, done = [], 0
+    t_start = time.perf_counter()
+    for _ in range(max(steps, 1)):
+        t0 = time.perf_counter()
+        for co in offs:
+            a.decode_chunk(co, out, 0)
+        times.append(time.perf_counter() - t0)
+        done += 1
+        if min_seconds and time.perf_counter() - t_start > min_seconds:
+            break
+    a.close()
+    cores = min(os.cpu_count() or 4, 16)   # the reference's thread cap (src/mc_archive.c:805-809)
+    gbs = nchunks * CHUNK / statistics.mean(times) / 1e9
+    return gbs, cores, done, times
+
+
+def build_reference_archive(path, vox_host, q):
+    from mcb200 import McLib
+    from oracle import REF_FAST_LIB
+    ref = McLib(REF_FAST_LIB, b200=False)
+    ref.L.mc_codec_init()
+    n = len(vox_host)
+    with ref.open(path, 256 * n, 256, 256, q) as a:
+        for c in range(n):
+            assert a.append_par(0, 0, 0, c, vox_host[c], q, 0) == 0
+
+
+def config(args, world):
+    return {"workload": f"batched chunk decode: {args.chunks} x 256^3 u8 chunks per GPU "
+                        f"({args.chunks * CHUNK / 2**30:.2f} GiB), q={args.q:g}, archive resident in HBM, "
+                        "one graph-captured decode plan per step",
+            "chunks_per_gpu": args.chunks, "q": args.q, "air_fraction": "30-60%",
+            "generator": "4-octave value noise (period 32) 40..220 + N(0,6^2), 2-octave air mask",
+            "l2": "flushed by a 256 MiB write between timed steps",
+            "parallelism": f"{world} x independent chunk shards"}
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args, d):
+    if d.rank != 0:
+        return None
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    vox = make_volumes(chunk_seeds(0, args.chunks), dev).cpu().numpy()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "ref.mca")
+        build_reference_archive(path, vox, args.q)
+        gbs, cores, done, times = reference_decode(path, args.chunks, args.q, args.steps, args.warmup)
+    ms = statistics.mean(times) * 1e3
+    sample = f"mc_archive_decode_chunk(nthreads=0) over all {args.chunks} chunks, {done} steps"
+    return {"metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": config(args, 1),
+            "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_b200(args, d):
+    from mcb200 import McLib, decode_chunk_blobs
+    lib = McLib.product()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    seeds = chunk_seeds(d.rank, args.chunks)
+    vox = make_volumes(seeds, dev)
+    td = tempfile.mkdtemp()
+    path = os.path.join(td, f"bench_{d.rank}.mca")
+    a = lib.open(path, 256 * args.chunks, 256, 256, args.q)
+    rc = a.append_chunks(0, [(0, 0, c) for c in range(args.chunks)], [vox[c].data_ptr() for c in range(args.chunks)],
+                         args.q, on_device=True)
+    assert rc == 0, "append failed"
+    del vox
+    offs = [a.chunk_offset(0, 0, 0, c) for c in range(args.chunks)]
+    out = torch.empty(args.chunks * CHUNK, dtype=torch.uint8, device=dev)
+    plan = a.plan_chunks(offs, out.data_ptr())
+    launches_per_step, blocks, payload = plan.info()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream()
+    for w in range(args.warmup):
+        flush.fill_(w & 0xFF)
+        plan.launch(s.cuda_stream)
+    torch.cuda.synchronize()
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(s)
+        plan.launch(s.cuda_stream)
+        ev[k][1].record(s)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    d.barrier()
+    torch.cuda.synchronize()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    ms = d.max(sum(step_ms)) / args.steps
+    decoded = d.world * args.chunks * CHUNK
+    value = decoded / (ms / 1e3) / 1e9
+
+    # per-stage timing: each kernel alone on the same stream, CUDA events
+    stage_ms = [0.0, 0.0]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        for stage in (0, 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            plan.launch_stage(stage, s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize()
+            stage_ms[stage] += e0.elapsed_time(e1) / args.steps
+
+    # bit-exactness spot check against the oracle on one chunk (rank 0)
+    exact = None
+    if d.rank == 0:
+        from oracle import Oracle
+        blob = bytes(blobs_of(path, [offs[0]])[0])
+        exact = bool(np.array_equal(out[:CHUNK].cpu().numpy(), Oracle().decode_chunk(blob)))
+
+    # plain per-call drop-in latency: mc_archive_decode_block on random blocks
+    rng = np.random.Generator(np.random.PCG64(d.rank))
+    lat = []
+    for _ in range(300):
+        c, bi = int(rng.integers(0, args.chunks)), int(rng.integers(0, 4096))
+        t0 = time.perf_counter()
+        a.decode_block(offs[c], bi >> 8, (bi >> 4) & 15, bi & 15)
+        lat.append((time.perf_counter() - t0) * 1e3)
+    lat = sorted(lat[20:])
+
+    # e2e: host blobs (pinned) -> host voxels (pinned) through the C ABI
+    blobs = blobs_of(path, offs)
+    pinned = [torch.from_numpy(b).pin_memory().numpy() for b in blobs]
+    hout = torch.empty(args.chunks * CHUNK, dtype=torch.uint8).pin_memory().numpy()
+    h2d = int(sum(b.size for b in pinned))
+    for _ in range(max(1, args.warmup // 2)):
+        decode_chunk_blobs(lib, pinned, hout)
+    d.barrier()
+    e2e_s = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        decode_chunk_blobs(lib, pinned, hout)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_value = decoded / (d.max(sum(e2e_s)) / args.steps) / 1e9
+    e2e_exact = bool(np.array_equal(hout[:CHUNK], out[:CHUNK].cpu().numpy())) if d.rank == 0 else None
+
+    plan.free()
+    a.close()
+
+    cpu = None
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        try:
+            gbs, cores, done, _ = reference_decode(path, args.chunks, args.q, 100, 1, min_seconds=8.0)
+            cpu = {"value": round(gbs, 4), "unit": "GB/s", "cores": cores, "kind": "reference",
+                   "sample": f"reference mc_archive_decode_chunk(nthreads=0) over the same {args.chunks}-chunk "
+                             f"archive, {done} passes (~8 s), sources built with the reference's default flags"}
+        except (FileNotFoundError, OSError) as e:
+            cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    os.remove(path)
+    os.rmdir(td)
+    if d.rank != 0:
+        return None
+
+    peak, peak_kind = hbm_peak()
+    ent_ms = stage_ms[0]
+    achieved = args.chunks * CHUNK / (ent_ms / 1e3) / 1e9
+    traffic = (ENTROPY_DRAM_BYTES_PER_CHUNK * args.chunks) if ENTROPY_DRAM_BYTES_PER_CHUNK else None
+    return {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": d.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded value-noise volumes; the reference's scroll CT data is not available offline)",
+        "config": config(args, d.world),
+        "gpu_launches": launches_per_step * args.steps,
+        "bit_exact_vs_oracle": exact,
+        "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": args.chunks * CHUNK, "api": "mc_b200_decode_chunk_blobs",
+                "bit_exact": e2e_exact},
+        "roofline": {"bound": "hbm", "kernel": "k_entropy (entropy decode stage)", "achieved": round(achieved, 2),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes_per_launch": args.chunks * CHUNK,
+                     "kernel_ms": round(ent_ms, 4), "reconstruct_ms": round(stage_ms[1], 4),
+                     "step_frac": round(value / d.world / peak, 4)},
+        "latency": {"api": "mc_archive_decode_block (plain per-call drop-in, host buffer)",
+                    "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[int(len(lat) * 0.99) - 1], 4)},
+        "blocks_per_step": blocks, "payload_bytes_per_step": payload,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+
+
+def main():
+    args = parse()
+    d = Dist("nccl" if torch.cuda.is_available() else "gloo")
+    try:
+        res = run_reference(args, d) if args.impl == "reference" else run_b200(args, d)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

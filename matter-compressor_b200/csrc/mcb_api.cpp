@@ -481,6 +481,15 @@ int mc_b200_plan_launch(mc_b200_plan *p, void *stream) {
     return cuda_ok(cudaGraphLaunch(p->exec, static_cast<cudaStream_t>(stream)), "graph launch") ? 0 : -1;
 }
 
+int mc_b200_plan_launch_stage(mc_b200_plan *p, int stage, void *stream) {
+    if (!p || stage < 0 || stage > 1) return -1;
+    if (p->a->d_base != p->mirror) {
+        set_error("decode plan is stale: the archive's device mirror moved since the plan was built");
+        return -1;
+    }
+    return decode_enqueue_stage(p->batch, p->cfg, stage, static_cast<cudaStream_t>(stream)) ? 0 : -1;
+}
+
 void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes) {
     if (launches) *launches = p ? p->launches : 0;
     if (blocks) *blocks = p ? p->blocks : 0;

@@ -204,9 +204,14 @@ bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t 
 }
 
 bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
+    return decode_enqueue_stage(B, cfg, -1, s);
+}
+
+bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaStream_t s) {
     Runtime *R = runtime();
     if (!R) return false;
-    if (!cuda_ok(cudaMemsetAsync(B.status.p, 0, 16, s), "memset")) return false;
+    const bool ent = stage != 1, rec = stage != 0;
+    if (ent && !cuda_ok(cudaMemsetAsync(B.status.p, 0, 16, s), "memset")) return false;
     for (auto &r : B.subs) {
         const int i0 = r.first, m = r.second - r.first;
         EntParams ep;
@@ -222,7 +227,7 @@ bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
         ep.qtab = R->d_qtab;
         ep.scan = R->d_scan;
         ep.status = B.status.as<uint32_t>();
-        if (!cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
+        if (ent && !cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
         RecParams rp;
         rp.items = B.items.as<DecItem>() + i0;
         rp.n = m;
@@ -231,7 +236,7 @@ bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
         rp.arena = B.arena.as<uint32_t>();
         rp.pool = B.pool.as<uint32_t>();
         rp.qtab = R->d_qtab;
-        if (!cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
+        if (rec && !cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
     }
     return true;
 }

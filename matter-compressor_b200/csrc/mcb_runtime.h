@@ -82,6 +82,8 @@ Lane *lane();
 
 bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s);
 bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s);
+// One stage only: 0 = status reset + entropy, 1 = reconstruction.
+bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaStream_t s);
 
 // Decodes n items whose src/dst are device addresses (host-side item array),
 // enqueued on stream s (null: the lane's stream); false on a launch error.

@@ -100,6 +100,7 @@ class McLib:
                 "mc_b200_read_regions_dev": (i, [vp, i, vp, i, lg, lg, lg, vp, sz, vp]),
                 "mc_b200_plan_decode_chunks": (vp, [vp, vp, i, vp, sz]),
                 "mc_b200_plan_launch": (i, [vp, vp]),
+                "mc_b200_plan_launch_stage": (i, [vp, i, vp]),
                 "mc_b200_plan_info": (None, [vp, C.POINTER(i), C.POINTER(lg), C.POINTER(u64)]),
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
@@ -311,6 +312,11 @@ class Plan:
 
     def launch(self, stream=None):
         rc = self.lib.L.mc_b200_plan_launch(self.p, C.c_void_p(stream) if stream else None)
+        self.lib.check()
+        return rc
+
+    def launch_stage(self, stage, stream=None):
+        rc = self.lib.L.mc_b200_plan_launch_stage(self.p, stage, C.c_void_p(stream) if stream else None)
         self.lib.check()
         return rc
 
