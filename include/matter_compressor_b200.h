@@ -161,6 +161,38 @@ void mc_b200_plan_free(mc_b200_plan *p);
 int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
                           const mc_u8 *const *vox, int vox_on_device, float q);
 
+/* Allocation-free block decode. This entry point has no counterpart in the
+ * reference; it is for callers that must not allocate memory: code running
+ * inside a memory pool's or allocator's own hooks (an allocation there would
+ * re-enter the allocator), and real-time loops that forbid allocation once
+ * started. It allocates nothing, on the device or the host: its work list,
+ * coefficient lists and tables live in one fixed 17.3 MiB array in device
+ * memory that the library declares statically.
+ *
+ * Decodes n payloads (as mc_dec_block takes them) already in DEVICE memory:
+ * payload i is d_payloads[h_offsets[i] .. h_offsets[i+1]) (h_offsets: n+1
+ * HOST values; an empty payload decodes to zeros), all at the one quality q
+ * of the payloads' context. Block i lands at d_out + i*4096 (z,y,x raster).
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream); the call returns before it ends.
+ *
+ * Limits: n <= 4096, and the sum over blocks of min(12288, 8*len_i + 64)
+ * <= 4194304 (about 512 KiB of payload); larger requests return -2 / -3 and
+ * must be split. d_payloads must be 8-byte aligned with 16 readable bytes
+ * after the last payload. Corrupt payloads decode as the reference decodes
+ * them, except that their spill past the fixed 1 MiB overflow area is cut
+ * short; no bad-block count is kept.
+ * Returns 0, or -1 (bad arguments), -2, -3 (limits), -4 (CUDA error); each
+ * failure prints one line to stderr.
+ *
+ * The first call on each device looks up the array's device address and
+ * uploads the constant tables, synchronously, with that device current: make
+ * it before any stream capture. All calls share the one array, so two calls
+ * whose work overlaps on the GPU (other streams, other host threads) race:
+ * order them on one stream or with events. */
+int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const uint64_t *h_offsets, int n,
+                                  float q, mc_u8 *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,7 @@ class McLib:
                 "mc_b200_plan_info": (None, [vp, C.POINTER(i), C.POINTER(lg), C.POINTER(u64)]),
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
+                "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
             })
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
