@@ -360,75 +360,108 @@ int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
 }
 
 // Blobs in host memory -> voxels in host memory, in groups of chunks.
+// Work items of one host blob whose bytes sit at d_blob on the device: block
+// payloads located through the blob's bitmap and length table
+// (src/mc_archive.h:175-206), bounded by the blob; every block of a blob that
+// is absent, short or malformed decodes to zeros. False only on a table error.
+static bool blob_items(const uint8_t *b, uint64_t bl, const uint8_t *d_blob, DecItem *it) {
+    if (!b || bl < (uint64_t)kBlobHdr) return true;
+    uint16_t fml;
+    memcpy(&fml, b + 12, 2);
+    const uint64_t bm_off = kBlobHdr + (uint64_t)fml;
+    if (bm_off + kBitmapBytes > bl) return true;
+    const uint8_t *bm = b + bm_off;
+    uint32_t np = 0;
+    for (int i = 0; i < kBitmapBytes; ++i) np += (uint32_t)__builtin_popcount(bm[i]);
+    const uint8_t *l16 = bm + kBitmapBytes;
+    if (bm_off + kBitmapBytes + 2ull * np > bl) return true;
+    float q;
+    memcpy(&q, b, 4);
+    const int slot = qslot(sanitize_q(q));
+    if (slot < 0) return false;
+    uint64_t pay = bm_off + kBitmapBytes + 2ull * np;
+    uint32_t k = 0;
+    for (int bi = 0; bi < kGrid3; ++bi) {
+        it[bi].qslot = (uint16_t)slot;
+        if (!((bm[bi >> 3] >> (bi & 7)) & 1)) continue;
+        uint16_t l;
+        memcpy(&l, l16 + 2 * k, 2);
+        ++k;
+        if (pay + l <= bl) {
+            it[bi].src = dptr(d_blob + pay);
+            it[bi].len = l;
+        }
+        pay += l;
+    }
+    return true;
+}
+
+// Host blobs in, host voxels out, as a two-slot pipeline over groups of
+// kBlobGroup chunks: while one slot's voxels travel device->host, the other
+// slot's blobs travel host->device and decode. A slot is reused once the
+// event recorded after its previous group's copy-out has fired.
 int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens, int n, mc_u8 *out,
                                size_t out_stride) {
     if (n < 0 || (n && (!blobs || !lens || !out))) return -1;
     Lane *L = lane();
     if (!L) return -1;
-    const int G = 16;
-    std::vector<DecItem> items;
-    for (int c0 = 0; c0 < n; c0 += G) {
-        const int g = std::min(G, n - c0);
+    constexpr int kBlobGroup = 8;
+    bool ok = blob_slot_ready(L->pipe[0]) && blob_slot_ready(L->pipe[1]);
+    uint32_t bad = 0;
+    int used[2] = {0, 0};
+    auto collect = [&](BlobSlot &S, int &u) {   // after S.done: count its cut-short blocks
+        if (u && S.batch.h_status.p) bad += *S.batch.h_status.as<uint32_t>();
+        u = 0;
+    };
+    for (int c0 = 0, gi = 0; ok && c0 < n; c0 += kBlobGroup, ++gi) {
+        BlobSlot &S = L->pipe[gi & 1];
+        const int g = std::min(kBlobGroup, n - c0);
+        ok = cuda_ok(cudaEventSynchronize(S.done), "event sync");
+        if (!ok) break;
+        collect(S, used[gi & 1]);
         uint64_t total = 0;
-        std::vector<uint64_t> at(g);
+        uint64_t at[kBlobGroup];
         for (int j = 0; j < g; ++j) {
             at[j] = total;
             total += blobs[c0 + j] ? ((lens[c0 + j] + 15) & ~15ull) : 0;
         }
-        if (!L->src.ensure(total + 64) || !L->out.ensure(kChunkBytes * g)) return -1;
-        items.assign((size_t)g * kGrid3, DecItem{});
-        for (int j = 0; j < g; ++j) {
+        DecodeBatch &B = S.batch;
+        const size_t ni = (size_t)g * kGrid3;
+        ok = S.src.ensure(total + 64) && S.out.ensure(kChunkBytes * g) && B.h_items.ensure(sizeof(DecItem) * ni) &&
+             B.h_status.ensure(16);
+        if (!ok) break;
+        DecItem *items = B.h_items.as<DecItem>();
+        for (int j = 0; j < g && ok; ++j) {
             const uint8_t *b = blobs[c0 + j];
-            const uint64_t bl = lens[c0 + j];
-            uint8_t *dchunk = L->out.as<uint8_t>() + kChunkBytes * j;
-            DecItem *it = &items[(size_t)j * kGrid3];
-            zero_chunk_items(dchunk, it);
-            if (!b || bl < (uint64_t)kBlobHdr) continue;
-            if (!cuda_ok(cudaMemcpyAsync(L->src.as<uint8_t>() + at[j], b, bl, cudaMemcpyHostToDevice, L->stream),
-                         "H2D blob"))
-                return -1;
-            // locate payloads (src/mc_archive.h:175-206), bounded by the blob
-            uint16_t fml;
-            memcpy(&fml, b + 12, 2);
-            const uint64_t bm_off = kBlobHdr + (uint64_t)fml;
-            if (bm_off + kBitmapBytes > bl) continue;
-            const uint8_t *bm = b + bm_off;
-            uint32_t np = 0;
-            for (int i = 0; i < kBitmapBytes; ++i) np += (uint32_t)__builtin_popcount(bm[i]);
-            const uint8_t *l16 = bm + kBitmapBytes;
-            if (bm_off + kBitmapBytes + 2ull * np > bl) continue;
-            float q;
-            memcpy(&q, b, 4);
-            const int slot = qslot(sanitize_q(q));
-            if (slot < 0) return -1;
-            uint64_t pay = bm_off + kBitmapBytes + 2ull * np;
-            uint32_t k = 0;
-            for (int bi = 0; bi < kGrid3; ++bi) {
-                it[bi].qslot = (uint16_t)slot;
-                if (!((bm[bi >> 3] >> (bi & 7)) & 1)) continue;
-                uint16_t l;
-                memcpy(&l, l16 + 2 * k, 2);
-                ++k;
-                if (pay + l <= bl) {
-                    it[bi].src = dptr(L->src.as<uint8_t>() + at[j] + pay);
-                    it[bi].len = l;
-                }
-                pay += l;
-            }
+            DecItem *it = items + (size_t)j * kGrid3;
+            zero_chunk_items(S.out.as<uint8_t>() + kChunkBytes * j, it);
+            if (b && lens[c0 + j] >= (uint64_t)kBlobHdr)
+                ok = cuda_ok(cudaMemcpyAsync(S.src.as<uint8_t>() + at[j], b, lens[c0 + j], cudaMemcpyHostToDevice,
+                                             S.stream), "H2D blob") &&
+                     blob_items(b, lens[c0 + j], S.src.as<uint8_t>() + at[j], it);
         }
-        if (!decode_items(*L, items.data(), (int)items.size())) return -1;
-        bool ok = true;
+        ok = ok && decode_prepare_staged(B, (int)ni, S.stream) && decode_enqueue(B, L->cfg, S.stream) &&
+             cuda_ok(cudaMemcpyAsync(B.h_status.p, B.status.p, 4, cudaMemcpyDeviceToHost, S.stream), "D2H status");
+        if (!ok) break;
         if (out_stride == kChunkBytes) {
-            ok = cuda_ok(cudaMemcpyAsync(out + kChunkBytes * c0, L->out.p, kChunkBytes * g, cudaMemcpyDeviceToHost,
-                                         L->stream), "D2H");
+            ok = cuda_ok(cudaMemcpyAsync(out + kChunkBytes * c0, S.out.p, kChunkBytes * g, cudaMemcpyDeviceToHost,
+                                         S.stream), "D2H");
         } else {
             for (int j = 0; j < g && ok; ++j)
-                ok = cuda_ok(cudaMemcpyAsync(out + out_stride * (c0 + j), L->out.as<uint8_t>() + kChunkBytes * j,
-                                             kChunkBytes, cudaMemcpyDeviceToHost, L->stream), "D2H");
+                ok = cuda_ok(cudaMemcpyAsync(out + out_stride * (c0 + j), S.out.as<uint8_t>() + kChunkBytes * j,
+                                             kChunkBytes, cudaMemcpyDeviceToHost, S.stream), "D2H");
         }
-        if (!ok || !finish(*L, nullptr)) return -1;
+        ok = ok && cuda_ok(cudaEventRecord(S.done, S.stream), "event record");
+        used[gi & 1] = 1;
     }
-    return 0;
+    for (int k = 0; k < 2; ++k) {   // drain both slots, also after an error
+        if (L->pipe[k].stream && cuda_ok(cudaStreamSynchronize(L->pipe[k].stream), "sync")) collect(L->pipe[k], used[k]);
+        else ok = false;
+    }
+    // the lane's status word reports the cut-short blocks of this call (mc_b200_last_bad_blocks)
+    if (ok && L->batch.status.ensure(16))
+        ok = cuda_ok(cudaMemcpy(L->batch.status.p, &bad, 4, cudaMemcpyHostToDevice), "status");
+    return ok ? 0 : -1;
 }
 
 // ============================================================ plans

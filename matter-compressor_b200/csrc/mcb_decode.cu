@@ -4,11 +4,13 @@
 // is a serial dependency chain per block (src/mc_codec.c:197-226), so the
 // parallelism is across blocks: every lane of a warp runs its own decoder and
 // the loop body decodes exactly one bin per lane per iteration (a flat state
-// machine), so lanes never wait on each other inside a block. The lane's 68
-// adaptive contexts sit in shared memory (context j of lane l at word
-// j*32+l: conflict-free), the scan table is staged once per CTA. Output per
-// block: a small header (dc, flags, extents) and a list of nonzero levels plus
-// corrections.
+// machine), so lanes never wait on each other inside a block. The per-bin
+// chain is kept short: the significance band is tracked by scan-position
+// boundaries and the density by a running count, so the only shared-memory
+// read on the chain is the context itself. The lane's adaptive contexts sit
+// in shared memory as 32-bit words (context j of lane l at word j*32+l:
+// conflict-free). Output per block: a small header (dc, flags) and a list of
+// nonzero levels plus corrections.
 //
 // Stage 2, k_reconstruct: one CTA (128 threads) per block. Dequantise into a
 // dense coefficient box bounded by the block's extents, then the three
@@ -31,44 +33,46 @@ namespace mcb {
 __constant__ float c_cos[16][16];
 
 // ---------------------------------------------------------------- stage 1
-// Lane states. The first four cover almost every bin of a block and share one
-// branch-light step (header bins, EOB prefix, significance, magnitude rungs
-// with their sign); the rest (EOB suffix, Exp-Golomb tails and their signs,
-// corrections) take a slow path entered a few times per block.
+// Lane states. F_SIG, F_MAG and F_SIGN are the bins of the coefficient loop
+// (over 95 % of a block's bins) and share one branch-light step; the rest are
+// entered a few times per block. The block header (flags, dc, EOB) is decoded
+// when a lane starts its block.
 enum : uint32_t {
-    F_HDR = 0,   // 10 context bins: flag0, flag1, dc bits 7..0 (contexts 0..9)
-    F_EOBP,      // EOB bit-length prefix, context 10+k
-    F_SIG,       // significance of scan position p
-    F_MAG,       // unary magnitude rung k, context 56+k (a zero rung takes the sign too)
-    S_SIGN,      // sign bypass after an Exp-Golomb magnitude
-    S_EOBS,      // EOB bits below the MSB (bypass, k bits)
+    F_SIG = 0,   // significance of scan position p: context sigb + min(cnt, 3)
+    F_MAG,       // unary magnitude rung k: context 56 + k
+    F_SIGN,      // sign (bypass) of the coefficient at p, magnitude m
     S_EGP,       // Exp-Golomb prefix (bypass)
     S_EGS,       // Exp-Golomb suffix (bypass, rem bits, 16 at a time)
     S_CSIGN,     // correction sign (bypass)
+    S_END,       // scan done: corrections or finished
     S_DONE,
     S_IDLE
 };
 enum : uint32_t { R_MAG = 0, R_CCOUNT, R_CGAP, R_CMAG };
+// Context slots per lane: the 68 adaptive contexts plus one scratch slot that
+// the sign bin reads and writes in place of a real context.
+constexpr int kCtxSlots = kNumCtx + 1;
+constexpr uint32_t kSignSlot = kNumCtx;
 
 struct LaneState {
     const uint8_t *src;
+    uint32_t *ent;             // the block's entries in the arena (first cap of them)
     uint32_t len, rpos;        // payload length, next byte index the window loads
     uint64_t wcur, wnext;      // byte window: current 8 bytes (wn left), next 8 bytes
     uint32_t wn;
     uint32_t code, range;
-    uint32_t st, k, lbase, p, eob, hist, hdr, mag;
+    uint32_t st, p, eob, hist, cnt, sigb, bend, band, k, m;
+    uint32_t hdr;              // flag0, flag1, dc bits 7..0 (10 bits, first bin highest)
     uint32_t nbits, rem, acc, ret;
     uint32_t ncorr, ccount, cpos, cneg;
-    uint32_t nent;             // entries written: coefficients, then 2 per correction
-    uint64_t base;
-    uint32_t cap, ovf, bad;
+    uint32_t nent, cap, ovf, bad;
     int item;
 };
 
 // Eight payload bytes from byte index pos (little-endian), zero past len.
-// Reads two aligned 8-byte words: every buffer that holds payloads keeps 64
-// readable bytes past its end and starts 256-byte aligned, so an aligned-down
-// address never precedes its buffer.
+// Reads two aligned 8-byte words: every buffer that holds payloads starts
+// 8-byte aligned and keeps 16 readable bytes past its last payload, so the
+// aligned words never leave the buffer.
 __device__ __forceinline__ uint64_t load8(const uint8_t *src, uint32_t len, uint32_t pos) {
     if (pos >= len) return 0ull;
     const uintptr_t addr = reinterpret_cast<uintptr_t>(src) + pos;
@@ -97,63 +101,121 @@ __device__ __forceinline__ uint32_t next_byte(LaneState &L) {
     return b;
 }
 
-__device__ __forceinline__ void put_entry(LaneState &L, const EntParams &P, uint32_t v) {
-    uint32_t j = L.nent;
+// Renormalise after a bin (src/mc_codec.c:202): the first byte by selects,
+// further bytes (rare: extreme probabilities) by the loop.
+__device__ __forceinline__ void renorm(LaneState &L) {
+    const bool need = L.range < (1u << 24);
+    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
+    L.code = need ? (L.code << 8) | b : L.code;
+    L.range = need ? L.range << 8 : L.range;
+    L.wcur = need ? L.wcur >> 8 : L.wcur;
+    L.wn -= need ? 1u : 0u;
+    if (L.wn == 0) refill(L);
+    while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
+}
+
+// One adaptive bin (src/mc_codec.c:198-204).
+__device__ __forceinline__ uint32_t ctx_bin(LaneState &L, uint32_t *cp) {
+    const uint32_t p0 = *cp;
+    const uint32_t r0 = (L.range >> 12) * p0;
+    const uint32_t bit = L.code >= r0 ? 1u : 0u;
+    L.code -= bit ? r0 : 0u;
+    L.range = bit ? L.range - r0 : r0;
+    *cp = bit ? p0 - (p0 >> 4) : p0 + ((4096u - p0) >> 4);
+    renorm(L);
+    return bit;
+}
+
+// nb bypass bits, 1 <= nb <= 16 (src/mc_codec.c:205,216-226).
+__device__ __forceinline__ uint32_t bypass_bits(LaneState &L, uint32_t nb) {
+    L.range >>= nb;
+    uint32_t q;
+    if (nb == 1) {
+        q = L.code >= L.range ? 1u : 0u;
+    } else {
+        q = L.code / L.range;
+        const uint32_t mx = (1u << nb) - 1u;
+        q = q > mx ? mx : q;
+    }
+    L.code -= q * L.range;
+    renorm(L);
+    return q;
+}
+
+// Appends one entry; false (stream cut short) when a corrupt stream also
+// exhausts the shared overflow pool.
+__device__ __forceinline__ bool put_entry(LaneState &L, const EntParams &P, uint32_t v) {
+    const uint32_t j = L.nent;
     if (j < L.cap) {
-        P.arena[L.base + j] = v;
+        L.ent[j] = v;
     } else {   // only corrupt streams get here
         if (L.ovf == 0xFFFFFFFFu) {
-            uint32_t need = kEntryMax - L.cap;
-            uint32_t off = atomicAdd(P.pool_used, need);
-            if ((uint64_t)off + need > P.pool_cap) { L.bad = 1; L.st = S_DONE; return; }
+            const uint32_t need = kEntryMax - L.cap;
+            const uint32_t off = atomicAdd(P.pool_used, need);
+            if ((uint64_t)off + need > P.pool_cap) { L.bad = 1; L.st = S_DONE; return false; }
             L.ovf = off;
         }
         P.pool[L.ovf + (j - L.cap)] = v;
     }
     L.nent = j + 1;
+    return true;
 }
 
-struct NextItem {   // descriptor of the lane's next block, loaded ahead of need
-    int slot;
-    uint64_t src, base;
-    uint32_t len, qslot;
-};
+// flags bit 1 (has corrections) is the second header bin
+__device__ __forceinline__ bool has_corr(const LaneState &L) { return (L.hdr >> 8) & 1; }
 
-__device__ __forceinline__ void prefetch_item(NextItem &N, const EntParams &P, int idx) {
-    N.slot = -1;
-    if (idx >= P.n) return;
-    const int slot = P.order ? (int)P.order[idx] : idx;
+// Scan position L.p became current. The last position before the EOB is
+// significant by definition and costs no bin (src/mc_codec.c:364); past the
+// EOB the coefficient loop ends.
+__device__ __forceinline__ void enter_position(LaneState &L) {
+    if (L.p + 1 >= L.eob) {
+        if (L.p + 1 == L.eob) {
+            L.hist = (L.hist << 1) | 1u;
+            L.cnt = L.cnt + 1u - ((L.hist >> 16) & 1u);
+            L.st = F_MAG;
+            L.k = 0;
+        } else {
+            L.st = S_END;
+        }
+    }
+}
+
+// Next scan position; the significance band changes at the precomputed
+// boundaries (bands are contiguous in scan order: the scan ascends in L1).
+__device__ __forceinline__ void advance(LaneState &L, const uint16_t *s_bend) {
+    const uint32_t p = ++L.p;
+    if (p == L.bend) { L.band++; L.sigb += 4; L.bend = s_bend[L.band]; }
+    enter_position(L);
+}
+
+// Starts block `slot`: contexts from the quality table, range decoder,
+// header bins, EOB (src/mc_codec.c:739-757, 321-327).
+__device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_bend,
+                                           int slot) {
     const DecItem &it = P.items[slot];
-    N.slot = slot;
-    N.src = it.src;
-    N.len = it.len;
-    N.qslot = it.qslot;
-    N.base = P.base[slot];
-}
-
-__device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uint16_t *ctx, const NextItem &N) {
-    L.item = N.slot;
-    L.src = reinterpret_cast<const uint8_t *>(N.src);
-    L.len = N.len;
-    L.base = N.base;
-    L.cap = entry_cap(N.len);
+    L.item = slot;
+    L.src = reinterpret_cast<const uint8_t *>(it.src);
+    L.len = it.len;
+    L.ent = P.arena + P.base[slot];
+    L.cap = entry_cap(L.len);
     L.ovf = 0xFFFFFFFFu;
     L.bad = 0;
     L.nent = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
     L.hdr = 0;
-    L.k = 0; L.lbase = kCtxFlag; L.p = 0; L.eob = 0; L.hist = 0; L.mag = 0;
     L.nbits = 0; L.rem = 0; L.acc = 0; L.ret = 0;
-    if (N.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
-    const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[N.qslot].ctx);
+    L.p = 0; L.eob = 0; L.hist = 0; L.cnt = 0; L.k = 0; L.m = 0;
+    L.band = 0; L.sigb = kCtxSig; L.bend = s_bend[0];
+    if (L.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
+    const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[it.qslot].ctx);
 #pragma unroll
     for (int j = 0; j < 9; ++j) {               // 72 u16 initial contexts
-        uint4 v = __ldg(q + j);
+        const uint4 v = __ldg(q + j);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             const int c = j * 8 + h * 2;
-            if (c < kNumCtx) ctx[c * 32] = (uint16_t)w[h];
-            if (c + 1 < kNumCtx) ctx[(c + 1) * 32] = (uint16_t)(w[h] >> 16);
+            if (c < kNumCtx) ctx[c * 32] = w[h] & 0xFFFFu;
+            if (c + 1 < kNumCtx) ctx[(c + 1) * 32] = w[h] >> 16;
         }
     }
     L.wcur = load8(L.src, L.len, 0);
@@ -163,7 +225,13 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
     L.range = 0xFFFFFFFFu;
     L.code = 0;
     for (int i = 0; i < 5; ++i) L.code = (L.code << 8) | next_byte(L);
-    L.st = F_HDR;
+    for (int i = 0; i < 10; ++i) L.hdr = (L.hdr << 1) | ctx_bin(L, ctx + (kCtxFlag + i) * 32);
+    uint32_t k = 0;
+    while (k < 13 && ctx_bin(L, ctx + (kCtxEob + k) * 32)) k++;
+    uint32_t eob = k < 2 ? k : (1u << (k - 1)) | bypass_bits(L, k - 1);
+    L.eob = eob > (uint32_t)kN3 ? (uint32_t)kN3 : eob;
+    L.st = F_SIG;
+    enter_position(L);
 }
 
 __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
@@ -181,31 +249,11 @@ __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
     if (L.bad) atomicAdd(P.status, 1u);
 }
 
-// flags bit 1 (has corrections) is the second header bin
-__device__ __forceinline__ bool has_corr(const LaneState &L) { return (L.hdr >> 8) & 1; }
-
-// Scan position p became current: past the end -> corrections or done; the
-// last position is significant by definition and costs no bin
-// (src/mc_codec.c:364).
-__device__ __forceinline__ void goto_position(LaneState &L) {
-    if (L.p >= L.eob) {
-        if (has_corr(L)) { L.st = S_EGP; L.nbits = 0; L.ret = R_CCOUNT; }
-        else L.st = S_DONE;
-    } else if (L.p == L.eob - 1) {
-        L.hist = (L.hist << 1) | 1u;
-        L.st = F_MAG;
-        L.k = 0;
-        L.lbase = kCtxMag;
-    } else {
-        L.st = F_SIG;
-    }
-}
-
 __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint32_t val) {
     switch (L.ret) {
     case R_MAG:
-        L.mag = 12u + val;            // 11 unary rungs + Exp-Golomb tail + 1
-        L.st = S_SIGN;                // the sign bypass follows
+        L.m = 12u + val;              // 11 unary rungs + Exp-Golomb tail + 1
+        L.st = F_SIGN;                // the sign bypass follows
         break;
     case R_CCOUNT: {
         uint32_t n = val + 1u;
@@ -220,12 +268,9 @@ __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint
         L.st = S_CSIGN;
         break;
     default: {   // R_CMAG
-        uint32_t m = val + 1u;
+        const uint32_t m = val + 1u;
         if (L.cpos >= (uint32_t)kN3) { L.st = S_DONE; break; }
-        put_entry(L, P, L.cpos);
-        if (L.st == S_DONE) break;
-        put_entry(L, P, L.cneg ? 0u - m : m);
-        if (L.st == S_DONE) break;
+        if (!put_entry(L, P, L.cpos) || !put_entry(L, P, L.cneg ? 0u - m : m)) break;
         L.ccount++;
         if (L.ccount == L.ncorr) L.st = S_DONE;
         else { L.st = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
@@ -234,29 +279,16 @@ __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint
     }
 }
 
-// Slow path: one bypass step of the rare states (src/mc_codec.c:205,216-238).
-__device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P, const uint32_t *s_scan) {
+// Slow path: one step of the rare states (src/mc_codec.c:205,216-238, 770-782).
+__device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P) {
     const uint32_t st = L.st;
-    const uint32_t nb = st == S_EOBS ? L.k : (st == S_EGS ? min(L.rem, 16u) : 1u);
-    L.range >>= nb;
-    uint32_t q;
-    if (nb == 1) {
-        q = L.code >= L.range ? 1u : 0u;
-    } else {
-        q = L.code / L.range;
-        const uint32_t mx = (1u << nb) - 1u;
-        q = q > mx ? mx : q;
+    if (st == S_END) {
+        if (has_corr(L)) { L.st = S_EGP; L.nbits = 0; L.ret = R_CCOUNT; }
+        else L.st = S_DONE;
+        return;
     }
-    L.code -= q * L.range;
-    while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
+    const uint32_t q = bypass_bits(L, st == S_EGS ? min(L.rem, 16u) : 1u);
     switch (st) {
-    case S_EOBS:
-        L.eob = (1u << L.k) | q;
-        if (L.eob > (uint32_t)kN3) L.eob = kN3;
-        L.p = 0;
-        L.hist = 0;
-        goto_position(L);
-        break;
     case S_EGP:   // Exp-Golomb prefix: count one-bits, capped on corrupt streams
         if (q) {
             if (++L.nbits >= (uint32_t)kEgCap) { L.bad = 1; L.st = S_DONE; }
@@ -266,15 +298,11 @@ __device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P, cons
             L.st = S_EGS; L.rem = L.nbits; L.acc = 0;
         }
         break;
-    case S_EGS:
+    case S_EGS: {
+        const uint32_t nb = min(L.rem, 16u);
         L.acc = (L.acc << nb) | q;
         L.rem -= nb;
         if (L.rem == 0) eg_return(L, P, ((1u << (L.nbits & 31)) | L.acc) - 1u);
-        break;
-    case S_SIGN: {
-        const uint32_t m = L.mag;
-        put_entry(L, P, (s_scan[L.p] & 0xFFFu) | ((q ? 0u - m : m) << 16));
-        if (L.st != S_DONE) { L.p++; goto_position(L); }
         break;
     }
     default:      // S_CSIGN
@@ -284,134 +312,91 @@ __device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P, cons
     }
 }
 
-// Renormalise after a bin: one byte by selects (the window always holds one),
-// further bytes (rare: extreme p0) by the loop (src/mc_codec.c:202).
-__device__ __forceinline__ void renorm(LaneState &L) {
-    const bool need = L.range < (1u << 24);
-    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
-    L.code = need ? (L.code << 8) | b : L.code;
-    L.range = need ? L.range << 8 : L.range;
-    L.wcur = need ? L.wcur >> 8 : L.wcur;
-    L.wn -= need ? 1u : 0u;
-    if (L.wn == 0) refill(L);
-    while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
-}
-
-// Scan position p became current (fast-path variant of goto_position).
-__device__ __forceinline__ void advance(LaneState &L) {
-    const uint32_t p = L.p;
-    const bool past = p >= L.eob;
-    const bool last = !past && p + 1 == L.eob;      // significant by definition (src/mc_codec.c:364)
-    L.hist = last ? (L.hist << 1) | 1u : L.hist;
-    L.k = 0;
-    L.lbase = kCtxMag;
-    L.nbits = 0;
-    L.ret = R_CCOUNT;
-    L.st = past ? (has_corr(L) ? (uint32_t)S_EGP : (uint32_t)S_DONE) : (last ? (uint32_t)F_MAG : (uint32_t)F_SIG);
-}
-
-// One context-coded bin of a lane in a fast state (src/mc_codec.c:198-204):
-// F_SIG uses the significance context of its scan position, the ladders
-// (header, EOB prefix, magnitude rungs) context lbase + k. A magnitude ended
-// by a zero rung takes its sign bypass bit in the same step.
-__device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint16_t *ctx, const uint32_t *s_scan) {
+// One bin of the coefficient loop. The significance bin of position p uses
+// context band*4 + min(popcount(last 16 significance flags), 3)
+// (src/mc_codec.c:249-259); magnitude rung k context 56+k
+// (src/mc_codec.c:268-275); the sign is a bypass bin (:205,369) computed by
+// the same instructions with r0 = range/2 and the scratch context slot.
+__device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_scan,
+                                          const uint16_t *s_bend) {
     const uint32_t st = L.st;
-    const bool is_sig = st == F_SIG;
-    const uint32_t sc = s_scan[L.p];                 // idx | (24 + 4*band) << 12
-    const uint32_t dens = min(__popc(L.hist & 0xFFFFu), 3);
-    const uint32_t cidx = is_sig ? (sc >> 12) + dens : L.lbase + L.k;
-    uint32_t p0 = ctx[cidx * 32];
-    const uint32_t r0 = (L.range >> 12) * p0;
-    const uint32_t bit = L.code >= r0 ? 1u : 0u;
-    L.code -= bit ? r0 : 0u;
-    L.range = bit ? L.range - r0 : r0;
-    ctx[cidx * 32] = (uint16_t)(bit ? p0 - (p0 >> 4) : p0 + ((4096u - p0) >> 4));
+    const bool sig = st == F_SIG, sign = st == F_SIGN;
+    const uint32_t c = sig ? L.sigb + min(L.cnt, 3u) : (sign ? kSignSlot : (uint32_t)kCtxMag + L.k);
+    uint32_t *cp = ctx + c * 32;
+    const uint32_t p0 = *cp;
+    const uint32_t r0 = sign ? L.range >> 1 : (L.range >> 12) * p0;
+    const bool bit = L.code >= r0;
+    L.code = bit ? L.code - r0 : L.code;
+    L.range = (bit && !sign) ? L.range - r0 : r0;
+    *cp = bit ? p0 - (p0 >> 4) : p0 + ((4096u - p0) >> 4);
     renorm(L);
 
-    if (is_sig) {
-        L.hist = (L.hist << 1) | bit;
-        if (bit) { L.st = F_MAG; L.k = 0; L.lbase = kCtxMag; }
-        else { L.p++; advance(L); }
-    } else if (st == F_MAG) {                        // 12 adaptive unary rungs (src/mc_codec.c:268-275)
-        if (bit) {
-            if (L.k < 11) L.k++;
-            else { L.st = S_EGP; L.nbits = 0; L.ret = R_MAG; }
-        } else {
-            // magnitude k+1 complete: sign bypass (src/mc_codec.c:205,369)
-            const uint32_t half = L.range >> 1;
-            const uint32_t neg = L.code >= half ? 1u : 0u;
-            L.code -= neg ? half : 0u;
-            L.range = half;
-            renorm(L);
-            const uint32_t m = L.k + 1;
-            put_entry(L, P, (sc & 0xFFFu) | ((neg ? 0u - m : m) << 16));
-            if (L.st != S_DONE) { L.p++; advance(L); }
-        }
-    } else if (st == F_HDR) {                        // flag0, flag1, dc bits 7..0
-        L.hdr = (L.hdr << 1) | bit;
-        if (++L.k == 10) { L.st = F_EOBP; L.k = 0; L.lbase = kCtxEob; }
-    } else {                                          // F_EOBP (src/mc_codec.c:321-327)
-        if (!(bit && ++L.k < 13)) {
-            if (L.k < 2) { L.eob = L.k; L.p = 0; L.hist = 0; advance(L); }
-            else { L.st = S_EOBS; L.k = L.k - 1; }
+    if (sig) {
+        L.hist = (L.hist << 1) | (bit ? 1u : 0u);
+        L.cnt = L.cnt + (bit ? 1u : 0u) - ((L.hist >> 16) & 1u);
+        L.k = 0;
+        if (bit) L.st = F_MAG;
+        else advance(L, s_bend);
+    } else if (!sign) {   // F_MAG, rung k
+        L.m = L.k + 1;
+        if (!bit) L.st = F_SIGN;
+        else if (L.k == 11) { L.st = S_EGP; L.nbits = 0; L.ret = R_MAG; }
+        else L.k++;
+    } else {              // F_SIGN: the coefficient is complete
+        const uint32_t m = L.m;
+        if (put_entry(L, P, (uint32_t)s_scan[L.p] | ((bit ? 0u - m : m) << 16))) {
+            L.st = F_SIG;
+            advance(L, s_bend);
         }
     }
 }
 
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
-    __shared__ uint32_t s_scan[kN3];   // raster idx | (24 + 4*band) << 12
-    __shared__ uint16_t s_ctx[WARPS][kNumCtx][32];
+    __shared__ uint16_t s_scan[kN3];   // scan position -> raster idx
+    __shared__ uint16_t s_bend[9];     // s_bend[b]: first scan position past band b
+    __shared__ uint32_t s_ctx[WARPS][kCtxSlots][32];
     for (int i = threadIdx.x; i < kN3; i += blockDim.x) {
-        const uint32_t v = P.scan[i];
-        s_scan[i] = (v & 0xFFFu) | ((uint32_t)kCtxSig + 4u * (v >> 12)) << 12;
+        const uint32_t v = P.scan[i], b = v >> 12;
+        s_scan[i] = (uint16_t)(v & 0xFFFu);
+        if (i > 0 && (P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
     }
+    if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint16_t *ctx = &s_ctx[warp][0][lane];
+    uint32_t *ctx = &s_ctx[warp][0][lane];
+    const int nlanes = gridDim.x * blockDim.x;
 
-    const int stride = gridDim.x * blockDim.x;
-    int next = blockIdx.x * blockDim.x + threadIdx.x;
+    // Work: the first ncoded entries of the processing order (longest payload
+    // first). Each lane starts with one block; later blocks come from a shared
+    // counter as lanes finish, so long and short blocks even out.
     LaneState L;
-    NextItem N;
     L.st = S_IDLE;
     L.item = -1;
-    prefetch_item(N, P, next);
-    next += stride;
-    // start the first block (skipping absent ones)
-    while (N.slot >= 0) {
-        lane_begin(L, P, ctx, N);
-        prefetch_item(N, P, next);
-        next += stride;
-        if (L.st != S_DONE) break;
-        lane_finish(L, P);
-        L.st = S_IDLE;
+    {
+        const int first = blockIdx.x * blockDim.x + threadIdx.x;
+        if (first < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[first] : first);
     }
 
-    // Inner loop: only the fast step, for as long as every live lane is in a
-    // fast state (idle lanes sit it out). Outer loop: the slow bypass steps and
-    // block switches, entered when some lane needs one. Every block ends after
-    // a bounded number of bins (finite scan, capped Exp-Golomb prefixes), so
-    // both loops terminate.
+    // Outer loop: block ends and slow steps of single lanes. Inner loop: two
+    // coefficient bins per live lane per round, for as long as no lane needs
+    // the outer loop (idle lanes sit it out). Every block ends after a bounded
+    // number of bins (finite scan, capped Exp-Golomb prefixes), and every lane
+    // fetches at most ncoded blocks, so both loops terminate.
     for (;;) {
-        while (__all_sync(0xFFFFFFFFu, L.st <= F_MAG || L.st == S_IDLE) &&
-               __any_sync(0xFFFFFFFFu, L.st != S_IDLE)) {
-            if (L.st <= F_MAG) fast_step(L, P, ctx, s_scan);
+        const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
+        if (idle == 0xFFFFFFFFu) break;
+        for (;;) {
+            if (L.st <= F_SIGN) fast_step(L, P, ctx, s_scan, s_bend);
+            if (L.st <= F_SIGN) fast_step(L, P, ctx, s_scan, s_bend);
+            if (__ballot_sync(0xFFFFFFFFu, L.st > F_SIGN) != idle) break;
         }
-        if (!__any_sync(0xFFFFFFFFu, L.st != S_IDLE)) break;
-        if (L.st <= F_MAG) fast_step(L, P, ctx, s_scan);
-        else if (L.st < S_DONE) slow_step(L, P, s_scan);
+        if (L.st > F_SIGN && L.st < S_DONE) slow_step(L, P);
         if (L.st == S_DONE) {
             lane_finish(L, P);
             L.st = S_IDLE;
-            while (N.slot >= 0) {
-                lane_begin(L, P, ctx, N);
-                prefetch_item(N, P, next);
-                next += stride;
-                if (L.st != S_DONE) break;
-                lane_finish(L, P);
-                L.st = S_IDLE;
-            }
+            const int nx = nlanes + (int)atomicAdd(P.status + 2, 1u);
+            if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[nx] : nx);
         }
     }
 }
@@ -726,11 +711,10 @@ static int num_sms() {
 }
 
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s) {
-    if (p.n <= 0) return cudaSuccess;
+    if (p.ncoded <= 0) return cudaSuccess;
     constexpr int W = 4;
-    int lanes = p.n;
-    int blocks = (lanes + W * 32 - 1) / (W * 32);
-    int cap = num_sms() * (cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 8);
+    int blocks = (p.ncoded + W * 32 - 1) / (W * 32);
+    int cap = num_sms() * (cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5);
     if (blocks > cap) blocks = cap;
     k_entropy<W><<<blocks, W * 32, 0, s>>>(p);
     return cudaGetLastError();

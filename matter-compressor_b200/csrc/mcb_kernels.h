@@ -9,7 +9,7 @@ namespace mcb {
 
 // Launch shape knobs, picked per quality by the autotuner.
 struct LaunchCfg {
-    int ent_ctas_per_sm = 6;   // entropy stage: CTAs of 4 warps per SM (<= 6: 75 regs, 34 KB smem)
+    int ent_ctas_per_sm = 5;   // entropy stage: CTAs of 4 warps per SM (<= 5: 44 KB smem)
     int rec_ctas_per_sm = 5;   // reconstruction stage: CTAs of 128 threads per SM (<= 5: 40 KB smem)
 };
 
@@ -17,6 +17,8 @@ struct EntParams {
     const DecItem *items;
     const uint32_t *order;     // optional processing order (by payload size), or null
     int n;
+    int ncoded;                // blocks to decode: the first ncoded of the order (the
+                               // rest are absent, len 0, and need no entropy stage)
     const uint64_t *base;      // per-item arena offset (entries)
     uint32_t *arena;
     EntHdr *hdr;
@@ -25,7 +27,8 @@ struct EntParams {
     uint32_t *pool_used;
     const QTab *qtab;
     const uint16_t *scan;      // scan position -> raster idx | band<<12
-    uint32_t *status;          // [0]: blocks whose stream was cut short
+    uint32_t *status;          // [0]: blocks whose stream was cut short, [1]: pool entries
+                               // used, [2]: work counter (all zero at launch)
 };
 
 struct RecParams {

@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(1024) k_noalloc_prepare(uint8_t *scratch, cons
     uint32_t *status = reinterpret_cast<uint32_t *>(scratch + kOffStatus);
     __shared__ uint32_t s_warp[32];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid < 4) status[tid] = 0;
+    if (tid < 4) status[tid] = 0;   // bad blocks, pool use, work counter
     uint32_t cap[4], sum = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -180,6 +180,7 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     ep.items = reinterpret_cast<const DecItem *>(sc + kOffItems);
     ep.order = nullptr;
     ep.n = n;
+    ep.ncoded = n;
     ep.base = reinterpret_cast<const uint64_t *>(sc + kOffBase);
     ep.arena = reinterpret_cast<uint32_t *>(sc + kOffArena);
     ep.hdr = reinterpret_cast<EntHdr *>(sc + kOffHdr);

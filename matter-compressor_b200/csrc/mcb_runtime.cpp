@@ -152,11 +152,15 @@ Lane *lane() {
 static constexpr uint64_t kArenaMaxEntries = 256ull << 20;   // 1 GiB of entries per sub-batch
 static constexpr uint32_t kPoolEntries = 4u << 20;           // overflow pool, 16 MiB
 
-bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s) {
+// Splits the items into sub-batches that fit the arena, writes each item's
+// arena offset (hb) and the entropy-stage order, and returns the largest
+// sub-batch's entry count. The order within a sub-batch is longest payload
+// first (counting sort by length), so the lanes of a warp decode blocks of
+// similar size and the per-lane totals balance (longest-processing-time-first).
+static uint64_t batch_layout(DecodeBatch &B, const DecItem *h_items, int n, uint64_t *hb, uint32_t *order) {
     B.n = n;
     B.subs.clear();
-    if (n <= 0) return true;
-    std::vector<uint64_t> hb((size_t)n);
+    B.coded.clear();
     uint64_t max_acc = 1;
     int i0 = 0;
     while (i0 < n) {
@@ -173,34 +177,74 @@ bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t 
         B.subs.emplace_back(i0, i1);
         i0 = i1;
     }
-    // entropy-stage order within each sub-batch: longest payload first
-    // (counting sort by length), so the lanes of a warp decode blocks of
-    // similar size and the per-lane totals balance (longest-processing-time-first)
-    std::vector<uint32_t> order((size_t)n);
-    {
-        std::vector<uint32_t> cnt(65536);
-        for (auto &r : B.subs) {
-            std::fill(cnt.begin(), cnt.end(), 0u);
-            auto key = [&](int i) { return 65535u - std::min<uint32_t>(h_items[i].len, 65535u); };
-            for (int i = r.first; i < r.second; ++i) cnt[key(i)]++;
-            uint32_t acc = 0;
-            for (auto &c : cnt) { uint32_t t = c; c = acc; acc += t; }
-            for (int i = r.first; i < r.second; ++i) order[r.first + cnt[key(i)]++] = (uint32_t)(i - r.first);
+    static thread_local std::vector<uint32_t> cnt;
+    cnt.resize(65536);
+    for (auto &r : B.subs) {
+        std::fill(cnt.begin(), cnt.end(), 0u);
+        auto key = [&](int i) { return 65535u - std::min<uint32_t>(h_items[i].len, 65535u); };
+        for (int i = r.first; i < r.second; ++i) cnt[key(i)]++;
+        uint32_t acc = 0;
+        for (auto &c : cnt) { uint32_t t = c; c = acc; acc += t; }
+        int coded = 0;
+        for (int i = r.first; i < r.second; ++i) {
+            order[r.first + cnt[key(i)]++] = (uint32_t)(i - r.first);
+            coded += h_items[i].len > 0;
         }
+        B.coded.push_back(coded);   // absent blocks sort last: the first `coded` entries have payloads
     }
-    if (!B.order.ensure(sizeof(uint32_t) * (size_t)n) || !B.items.ensure(sizeof(DecItem) * (size_t)n) ||
-        !B.base.ensure(sizeof(uint64_t) * (size_t)n) ||
-        !B.hdr.ensure(sizeof(EntHdr) * (size_t)n) || !B.arena.ensure(sizeof(uint32_t) * max_acc) ||
-        !B.pool.ensure(sizeof(uint32_t) * kPoolEntries) || !B.status.ensure(16))
-        return false;
-    // synchronous copies: the host arrays may be pageable and short-lived
-    return cuda_ok(cudaMemcpyAsync(B.items.p, h_items, sizeof(DecItem) * (size_t)n, cudaMemcpyHostToDevice, s),
+    return max_acc;
+}
+
+static bool batch_buffers(DecodeBatch &B, int n, uint64_t max_acc) {
+    return B.order.ensure(sizeof(uint32_t) * (size_t)n) && B.items.ensure(sizeof(DecItem) * (size_t)n) &&
+           B.base.ensure(sizeof(uint64_t) * (size_t)n) && B.hdr.ensure(sizeof(EntHdr) * (size_t)n) &&
+           B.arena.ensure(sizeof(uint32_t) * max_acc) && B.pool.ensure(sizeof(uint32_t) * kPoolEntries) &&
+           B.status.ensure(16);
+}
+
+static bool batch_upload(DecodeBatch &B, const DecItem *items, const uint32_t *order, const uint64_t *hb, int n,
+                         cudaStream_t s) {
+    return cuda_ok(cudaMemcpyAsync(B.items.p, items, sizeof(DecItem) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D items") &&
-           cuda_ok(cudaMemcpyAsync(B.order.p, order.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s),
+           cuda_ok(cudaMemcpyAsync(B.order.p, order, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D order") &&
-           cuda_ok(cudaMemcpyAsync(B.base.p, hb.data(), sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s),
-                   "H2D base") &&
+           cuda_ok(cudaMemcpyAsync(B.base.p, hb, sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s),
+                   "H2D base");
+}
+
+bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s) {
+    B.n = n;
+    B.subs.clear();
+    if (n <= 0) return true;
+    std::vector<uint64_t> hb((size_t)n);
+    std::vector<uint32_t> order((size_t)n);
+    const uint64_t max_acc = batch_layout(B, h_items, n, hb.data(), order.data());
+    // synchronous copies: the host arrays may be pageable and short-lived
+    return batch_buffers(B, n, max_acc) && batch_upload(B, h_items, order.data(), hb.data(), n, s) &&
            cuda_ok(cudaStreamSynchronize(s), "sync");
+}
+
+bool decode_prepare_staged(DecodeBatch &B, int n, cudaStream_t s) {
+    B.n = n;
+    B.subs.clear();
+    if (n <= 0) return true;
+    if (!B.h_order.ensure(sizeof(uint32_t) * (size_t)n) || !B.h_base.ensure(sizeof(uint64_t) * (size_t)n))
+        return false;
+    const DecItem *items = B.h_items.as<DecItem>();
+    const uint64_t max_acc = batch_layout(B, items, n, B.h_base.as<uint64_t>(), B.h_order.as<uint32_t>());
+    return batch_buffers(B, n, max_acc) &&
+           batch_upload(B, items, B.h_order.as<uint32_t>(), B.h_base.as<uint64_t>(), n, s);
+}
+
+BlobSlot::~BlobSlot() {
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+bool blob_slot_ready(BlobSlot &S) {
+    if (S.stream) return true;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking), "stream")) return false;
+    return cuda_ok(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming), "event");
 }
 
 bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
@@ -212,12 +256,13 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
     if (!R) return false;
     const bool ent = stage != 1, rec = stage != 0;
     if (ent && !cuda_ok(cudaMemsetAsync(B.status.p, 0, 16, s), "memset")) return false;
-    for (auto &r : B.subs) {
-        const int i0 = r.first, m = r.second - r.first;
+    for (size_t si = 0; si < B.subs.size(); ++si) {
+        const int i0 = B.subs[si].first, m = B.subs[si].second - B.subs[si].first;
         EntParams ep;
         ep.items = B.items.as<DecItem>() + i0;
         ep.order = B.order.as<uint32_t>() + i0;
         ep.n = m;
+        ep.ncoded = B.coded[si];
         ep.base = B.base.as<uint64_t>() + i0;
         ep.arena = B.arena.as<uint32_t>();
         ep.hdr = B.hdr.as<EntHdr>() + i0;
@@ -227,6 +272,8 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         ep.qtab = R->d_qtab;
         ep.scan = R->d_scan;
         ep.status = B.status.as<uint32_t>();
+        // each sub-batch's entropy launch starts its work counter at zero
+        if (ent && si > 0 && !cuda_ok(cudaMemsetAsync(B.status.as<uint32_t>() + 2, 0, 4, s), "memset")) return false;
         if (ent && !cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
         RecParams rp;
         rp.items = B.items.as<DecItem>() + i0;

@@ -63,8 +63,19 @@ int qslot(float q);
 // two stages (capturable into a CUDA graph).
 struct DecodeBatch {
     DevBuf items, order, base, hdr, arena, pool, status;
+    HostBuf h_items, h_order, h_base, h_status;   // pinned staging of decode_prepare_staged
     int n = 0;
     std::vector<std::pair<int, int>> subs;   // [i0, i1) ranges that fit the arena
+    std::vector<int> coded;                  // per sub-batch: items with a payload
+};
+// One stage of the host-blob decode pipeline: its own stream, batch and
+// device buffers, reused once the event of its previous group has fired.
+struct BlobSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    DecodeBatch batch;
+    DevBuf src, out;
+    ~BlobSlot();
 };
 // Per-thread execution resources: a stream and reusable buffers.
 struct Lane {
@@ -76,11 +87,19 @@ struct Lane {
     DevBuf b_scratch, b_lens16, b_bitmap, b_fmap, b_fml, b_np, b_len, b_off, b_q, blobs;
     HostBuf h_items, h_base, h_stage, h_misc;
     LaunchCfg cfg;
+    BlobSlot pipe[2];
     ~Lane();
 };
 Lane *lane();
 
 bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t s);
+// decode_prepare without any host synchronisation: the n items are already in
+// B.h_items (pinned), order and offsets are built in B's pinned staging, and
+// every upload is asynchronous on s. The caller guarantees that the batch's
+// previous use has completed.
+bool decode_prepare_staged(DecodeBatch &B, int n, cudaStream_t s);
+// Creates the stream and event of a pipeline slot on first use.
+bool blob_slot_ready(BlobSlot &S);
 bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s);
 // One stage only: 0 = status reset + entropy, 1 = reconstruction.
 bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaStream_t s);

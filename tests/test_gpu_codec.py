@@ -50,6 +50,28 @@ def test_chunk_blobs_decode_golden(gpu, golden_chunks):
         assert sha(out[i * CHUNK:(i + 1) * CHUNK]) == g["decoded_sha"][i], g["names"][i]
 
 
+def test_chunk_blobs_pipeline(gpu, golden_chunks):
+    """More blobs than one pipeline group (three groups over both slots), a
+    missing blob, and a padded output stride: every chunk still matches."""
+    import ctypes as C
+    g = golden_chunks
+    blobs = [g["blobs"][g["offs"][i]:g["offs"][i + 1]] for i in range(len(g["offs"]) - 1)]
+    want = [str(s) for s in g["decoded_sha"]]
+    seq = [(i * 5) % len(blobs) for i in range(19)]
+    arrs = [blobs[i] for i in seq]
+    ptrs = (C.c_void_p * len(arrs))(*[(a.ctypes.data if a.size else None) for a in arrs])
+    lens = np.asarray([a.size for a in arrs], np.uint64)
+    stride = CHUNK + 4096
+    out = np.full(len(arrs) * stride, 0x5A, np.uint8)
+    rc = gpu.L.mc_b200_decode_chunk_blobs(C.cast(ptrs, C.c_void_p), lens.ctypes.data, len(arrs), out.ctypes.data,
+                                          stride)
+    assert rc == 0
+    for j, i in enumerate(seq):
+        assert sha(out[j * stride:j * stride + CHUNK]) == want[i], (j, g["names"][i])
+        assert np.all(out[j * stride + CHUNK:(j + 1) * stride] == 0x5A)
+    assert gpu.L.mc_b200_last_bad_blocks() == 0
+
+
 def _append_sequence(lib, path):
     offs = []
     with lib.open(path, 1024, 1024, 1024, 6.0) as a:
