@@ -33,15 +33,15 @@ namespace mcb {
 __constant__ float c_cos[16][16];
 
 // ---------------------------------------------------------------- stage 1
-// Lane states. F_SIG, F_MAG and F_SIGN are the bins of the coefficient loop
-// (over 95 % of a block's bins) and share one branch-light step; the rest are
-// entered a few times per block. The block header (flags, dc, EOB) is decoded
-// when a lane starts its block.
+// Lane states. F_SIG, F_MAG, F_SIGN and F_EGP cover nearly every bin of a
+// block and share one branch-light step; the rest are entered a few times per
+// block. The block header (flags, dc, EOB) is decoded when a lane starts its
+// block.
 enum : uint32_t {
     F_SIG = 0,   // significance of scan position p: context sigb + min(cnt, 3)
     F_MAG,       // unary magnitude rung k: context 56 + k
     F_SIGN,      // sign (bypass) of the coefficient at p, magnitude m
-    S_EGP,       // Exp-Golomb prefix (bypass)
+    F_EGP,       // Exp-Golomb prefix (bypass): k counts 12 + the one-bits so far
     S_EGS,       // Exp-Golomb suffix (bypass, rem bits, 16 at a time)
     S_CSIGN,     // correction sign (bypass)
     S_END,       // scan done: corrections or finished
@@ -50,67 +50,59 @@ enum : uint32_t {
 };
 enum : uint32_t { R_MAG = 0, R_CCOUNT, R_CGAP, R_CMAG };
 // Context slots per lane: the 68 adaptive contexts plus one scratch slot that
-// the sign bin reads and writes in place of a real context.
+// bypass bins read and write in place of a real context.
 constexpr int kCtxSlots = kNumCtx + 1;
 constexpr uint32_t kSignSlot = kNumCtx;
+// Exp-Golomb prefixes count in k from this base (the magnitude ladder hands
+// over at its 12th rung with k = 12).
+constexpr uint32_t kEgBase = 12;
+// Byte-permute selector that shifts code left one byte and brings in byte i
+// of the window: result = {code.b2, code.b1, code.b0, w.b[i]}; i = sel - kSel0.
+constexpr uint32_t kSel0 = 0x2104u;
 
 struct LaneState {
-    const uint8_t *src;
+    const uint8_t *abase;      // payload start rounded down to 4 bytes
     uint32_t *ent;             // the block's entries in the arena (first cap of them)
-    uint32_t len, rpos;        // payload length, next byte index the window loads
-    uint64_t wcur, wnext;      // byte window: current 8 bytes (wn left), next 8 bytes
-    uint32_t wn;
+    uint32_t len, off0;        // payload length, payload start - abase
+    uint32_t w, nxt, sel, jn;  // window word, next word, byte selector, index of the next word
     uint32_t code, range;
-    uint32_t st, p, eob, hist, cnt, sigb, bend, band, k, m;
+    uint32_t st, p, eob, cnt, hist, sigb, band, bend, stop, k, m;
+    uint32_t cc, pc;           // context slot of the next bin and its probability (coefficient loop)
     uint32_t hdr;              // flag0, flag1, dc bits 7..0 (10 bits, first bin highest)
-    uint32_t nbits, rem, acc, ret;
+    uint32_t rem, acc, ret;
     uint32_t ncorr, ccount, cpos, cneg;
     uint32_t nent, cap, ovf, bad;
     int item;
 };
 
-// Eight payload bytes from byte index pos (little-endian), zero past len.
-// Reads two aligned 8-byte words: every buffer that holds payloads starts
-// 8-byte aligned and keeps 16 readable bytes past its last payload, so the
-// aligned words never leave the buffer.
-__device__ __forceinline__ uint64_t load8(const uint8_t *src, uint32_t len, uint32_t pos) {
-    if (pos >= len) return 0ull;
-    const uintptr_t addr = reinterpret_cast<uintptr_t>(src) + pos;
-    const uint64_t *a = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
-    const uint32_t sh = (uint32_t)(addr & 7) * 8u;
-    const uint64_t lo = __ldg(a), hi = __ldg(a + 1);
-    uint64_t w = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-    const uint32_t avail = len - pos;
-    if (avail < 8) w &= (1ull << (8 * avail)) - 1ull;
-    return w;
+// Payload word j (bytes 4j-off0 .. 4j-off0+3 of the payload), bytes past the
+// payload read as zero (src/mc_codec.c:96). Loads are 4-byte aligned and never
+// start past the word holding the payload's last byte.
+__device__ __forceinline__ uint32_t load_word(const LaneState &L, uint32_t j) {
+    const int first = (int)(4 * j) - (int)L.off0;   // payload index of the word's byte 0
+    if (first >= (int)L.len) return 0u;
+    uint32_t v = __ldg(reinterpret_cast<const uint32_t *>(L.abase) + j);
+    const int avail = (int)L.len - first;
+    if (avail < 4) v &= (1u << (8 * avail)) - 1u;
+    return v;
 }
 
 __device__ __forceinline__ void refill(LaneState &L) {
-    L.wcur = L.wnext;
-    L.wn = 8;
-    L.wnext = load8(L.src, L.len, L.rpos);
-    L.rpos += 8;
+    L.w = L.nxt;
+    L.sel = kSel0;
+    L.nxt = load_word(L, ++L.jn);
 }
 
-// The window always holds at least one unread byte: consuming the last one
-// refills it at once (invariant wn >= 1 between calls).
+// One payload byte (slow paths). The window always holds an unread byte:
+// consuming the last one refills it at once.
 __device__ __forceinline__ uint32_t next_byte(LaneState &L) {
-    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
-    L.wcur >>= 8;
-    if (--L.wn == 0) refill(L);
+    const uint32_t b = (L.w >> (8 * (L.sel - kSel0))) & 0xFFu;
+    if (++L.sel == kSel0 + 4) refill(L);
     return b;
 }
 
-// Renormalise after a bin (src/mc_codec.c:202): the first byte by selects,
-// further bytes (rare: extreme probabilities) by the loop.
+// Renormalise (src/mc_codec.c:202).
 __device__ __forceinline__ void renorm(LaneState &L) {
-    const bool need = L.range < (1u << 24);
-    const uint32_t b = (uint32_t)L.wcur & 0xFFu;
-    L.code = need ? (L.code << 8) | b : L.code;
-    L.range = need ? L.range << 8 : L.range;
-    L.wcur = need ? L.wcur >> 8 : L.wcur;
-    L.wn -= need ? 1u : 0u;
-    if (L.wn == 0) refill(L);
     while (L.range < (1u << 24)) { L.code = (L.code << 8) | next_byte(L); L.range <<= 8; }
 }
 
@@ -161,13 +153,22 @@ __device__ __forceinline__ bool put_entry(LaneState &L, const EntParams &P, uint
     return true;
 }
 
+// Context slot of the bin the lane's state asks for next and its current
+// value; bypass states use the scratch slot.
+__device__ __forceinline__ void load_ctx(LaneState &L, const uint32_t *ctx) {
+    L.cc = L.st == F_SIG ? L.sigb + min(L.cnt, 3u) : (L.st == F_MAG ? (uint32_t)kCtxMag + L.k : kSignSlot);
+    L.pc = ctx[L.cc * 32];
+}
+
 // flags bit 1 (has corrections) is the second header bin
 __device__ __forceinline__ bool has_corr(const LaneState &L) { return (L.hdr >> 8) & 1; }
 
-// Scan position L.p became current. The last position before the EOB is
-// significant by definition and costs no bin (src/mc_codec.c:364); past the
-// EOB the coefficient loop ends.
-__device__ __forceinline__ void enter_position(LaneState &L) {
+// Scan position L.p is current and L.p >= L.stop: a band change and/or the
+// end of the scan. The last position before the EOB is significant by
+// definition and costs no bin (src/mc_codec.c:364); past the EOB the
+// coefficient loop ends.
+__device__ __forceinline__ void position_event(LaneState &L, const uint32_t *ctx, const uint16_t *s_bend) {
+    while (L.p >= L.bend) { L.band++; L.sigb += 4; L.bend = s_bend[L.band]; }
     if (L.p + 1 >= L.eob) {
         if (L.p + 1 == L.eob) {
             L.hist = (L.hist << 1) | 1u;
@@ -178,14 +179,8 @@ __device__ __forceinline__ void enter_position(LaneState &L) {
             L.st = S_END;
         }
     }
-}
-
-// Next scan position; the significance band changes at the precomputed
-// boundaries (bands are contiguous in scan order: the scan ascends in L1).
-__device__ __forceinline__ void advance(LaneState &L, const uint16_t *s_bend) {
-    const uint32_t p = ++L.p;
-    if (p == L.bend) { L.band++; L.sigb += 4; L.bend = s_bend[L.band]; }
-    enter_position(L);
+    L.stop = min(L.bend, L.eob - 1);   // eob >= 1 here (eob == 0 never enters the scan)
+    load_ctx(L, ctx);
 }
 
 // Starts block `slot`: contexts from the quality table, range decoder,
@@ -194,7 +189,9 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
                                            int slot) {
     const DecItem &it = P.items[slot];
     L.item = slot;
-    L.src = reinterpret_cast<const uint8_t *>(it.src);
+    const uintptr_t src = (uintptr_t)it.src;
+    L.abase = reinterpret_cast<const uint8_t *>(src & ~(uintptr_t)3);
+    L.off0 = (uint32_t)(src & 3);
     L.len = it.len;
     L.ent = P.arena + P.base[slot];
     L.cap = entry_cap(L.len);
@@ -202,9 +199,9 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
     L.bad = 0;
     L.nent = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
     L.hdr = 0;
-    L.nbits = 0; L.rem = 0; L.acc = 0; L.ret = 0;
+    L.rem = 0; L.acc = 0; L.ret = R_MAG;
     L.p = 0; L.eob = 0; L.hist = 0; L.cnt = 0; L.k = 0; L.m = 0;
-    L.band = 0; L.sigb = kCtxSig; L.bend = s_bend[0];
+    L.band = 0; L.sigb = kCtxSig; L.bend = s_bend[0]; L.stop = 0;
     if (L.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
     const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[it.qslot].ctx);
 #pragma unroll
@@ -218,20 +215,21 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
             if (c + 1 < kNumCtx) ctx[(c + 1) * 32] = w[h] >> 16;
         }
     }
-    L.wcur = load8(L.src, L.len, 0);
-    L.wnext = load8(L.src, L.len, 8);
-    L.wn = 8;
-    L.rpos = 16;
+    L.w = load_word(L, 0);
+    L.sel = kSel0 + L.off0;
+    L.jn = 1;
+    L.nxt = load_word(L, 1);
     L.range = 0xFFFFFFFFu;
     L.code = 0;
     for (int i = 0; i < 5; ++i) L.code = (L.code << 8) | next_byte(L);
     for (int i = 0; i < 10; ++i) L.hdr = (L.hdr << 1) | ctx_bin(L, ctx + (kCtxFlag + i) * 32);
     uint32_t k = 0;
     while (k < 13 && ctx_bin(L, ctx + (kCtxEob + k) * 32)) k++;
-    uint32_t eob = k < 2 ? k : (1u << (k - 1)) | bypass_bits(L, k - 1);
+    const uint32_t eob = k < 2 ? k : (1u << (k - 1)) | bypass_bits(L, k - 1);
     L.eob = eob > (uint32_t)kN3 ? (uint32_t)kN3 : eob;
+    if (L.eob == 0) { L.st = S_END; return; }
     L.st = F_SIG;
-    enter_position(L);
+    position_event(L, ctx, s_bend);
 }
 
 __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
@@ -249,6 +247,10 @@ __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
     if (L.bad) atomicAdd(P.status, 1u);
 }
 
+__device__ __forceinline__ void eg_start(LaneState &L, uint32_t ret) {
+    L.st = F_EGP; L.k = kEgBase; L.ret = ret;
+}
+
 __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint32_t val) {
     switch (L.ret) {
     case R_MAG:
@@ -259,8 +261,7 @@ __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint
         uint32_t n = val + 1u;
         if (n > (uint32_t)kN3) n = kN3;
         L.ncorr = n; L.ccount = 0; L.cpos = 0;
-        if (n == 0) L.st = S_DONE;
-        else { L.st = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
+        eg_start(L, R_CGAP);
         break;
     }
     case R_CGAP:
@@ -273,93 +274,137 @@ __device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint
         if (!put_entry(L, P, L.cpos) || !put_entry(L, P, L.cneg ? 0u - m : m)) break;
         L.ccount++;
         if (L.ccount == L.ncorr) L.st = S_DONE;
-        else { L.st = S_EGP; L.nbits = 0; L.ret = R_CGAP; }
+        else eg_start(L, R_CGAP);
         break;
     }
     }
 }
 
-// Slow path: one step of the rare states (src/mc_codec.c:205,216-238, 770-782).
+// Slow path: one step of the rare states (src/mc_codec.c:216-238, 770-782).
 __device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P) {
     const uint32_t st = L.st;
     if (st == S_END) {
-        if (has_corr(L)) { L.st = S_EGP; L.nbits = 0; L.ret = R_CCOUNT; }
+        if (has_corr(L)) eg_start(L, R_CCOUNT);
         else L.st = S_DONE;
         return;
     }
-    const uint32_t q = bypass_bits(L, st == S_EGS ? min(L.rem, 16u) : 1u);
-    switch (st) {
-    case S_EGP:   // Exp-Golomb prefix: count one-bits, capped on corrupt streams
-        if (q) {
-            if (++L.nbits >= (uint32_t)kEgCap) { L.bad = 1; L.st = S_DONE; }
-        } else if (L.nbits == 0) {
-            eg_return(L, P, 0);
-        } else {
-            L.st = S_EGS; L.rem = L.nbits; L.acc = 0;
-        }
-        break;
-    case S_EGS: {
+    if (st == S_EGS) {
         const uint32_t nb = min(L.rem, 16u);
-        L.acc = (L.acc << nb) | q;
+        L.acc = (L.acc << nb) | bypass_bits(L, nb);
         L.rem -= nb;
-        if (L.rem == 0) eg_return(L, P, ((1u << (L.nbits & 31)) | L.acc) - 1u);
-        break;
+        if (L.rem == 0) {
+            const uint32_t nbits = L.k - kEgBase;
+            eg_return(L, P, ((1u << (nbits & 31)) | L.acc) - 1u);
+        }
+    } else {      // S_CSIGN
+        L.cneg = bypass_bits(L, 1);
+        eg_start(L, R_CMAG);
     }
-    default:      // S_CSIGN
-        L.cneg = q;
-        L.st = S_EGP; L.nbits = 0; L.ret = R_CMAG;
-        break;
-    }
+}
+
+// Predicated shared / global stores (one instruction each, no branch).
+__device__ __forceinline__ void sts_if(bool pred, uint32_t *p, uint32_t v) {
+    asm volatile("{.reg .pred q; setp.ne.u32 q, %2, 0; @q st.shared.u32 [%0], %1;}"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v), "r"((uint32_t)pred) : "memory");
+}
+__device__ __forceinline__ void stg_if(bool pred, uint32_t *p, uint32_t v) {
+    asm volatile("{.reg .pred q; setp.ne.u32 q, %2, 0; @q st.global.u32 [%0], %1;}"
+                 :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
 }
 
 // One bin of the coefficient loop. The significance bin of position p uses
 // context band*4 + min(popcount(last 16 significance flags), 3)
 // (src/mc_codec.c:249-259); magnitude rung k context 56+k
-// (src/mc_codec.c:268-275); the sign is a bypass bin (:205,369) computed by
-// the same instructions with r0 = range/2 and the scratch context slot.
-__device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_scan,
-                                          const uint16_t *s_bend) {
+// (src/mc_codec.c:268-275); signs and Exp-Golomb prefix bits are bypass bins
+// (:205,229-238,369) computed by the same instructions with r0 = range/2 and
+// the scratch context slot.
+// The step is software-pipelined: the bin's context value (pc, slot cc) was
+// fetched during the previous step, and this step fetches both candidate
+// contexts of the next bin (one per value of this bin) before it decodes, so
+// the shared-memory round trip overlaps the arithmetic; a next context equal
+// to this bin's takes the freshly updated value instead. The common path is
+// straight-line code of selects and predicated stores, so a warp whose lanes
+// sit in different states issues one instruction stream; rare events (window
+// refill, a second renormalisation byte, band change, end of scan, end of an
+// Exp-Golomb prefix, entry-list overflow) share one branch. A lane in any
+// other state passes through unchanged.
+__device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_bend) {
     const uint32_t st = L.st;
-    const bool sig = st == F_SIG, sign = st == F_SIGN;
-    const uint32_t c = sig ? L.sigb + min(L.cnt, 3u) : (sign ? kSignSlot : (uint32_t)kCtxMag + L.k);
-    uint32_t *cp = ctx + c * 32;
-    const uint32_t p0 = *cp;
-    const uint32_t r0 = sign ? L.range >> 1 : (L.range >> 12) * p0;
-    const bool bit = L.code >= r0;
-    L.code = bit ? L.code - r0 : L.code;
-    L.range = (bit && !sign) ? L.range - r0 : r0;
-    *cp = bit ? p0 - (p0 >> 4) : p0 + ((4096u - p0) >> 4);
-    renorm(L);
+    const bool live = st <= F_EGP;
+    const bool is_sig = st == F_SIG, is_mag = st == F_MAG, is_sign = st == F_SIGN, is_egp = st == F_EGP;
+    const bool is_byp = is_sign | is_egp;
+    // candidate contexts of the next bin: c0 if this bin is 0, c1 if it is 1
+    const uint32_t out = (L.hist >> 15) & 1u;
+    const uint32_t k1 = L.k + 1u;
+    const uint32_t sig_next = L.sigb + min(L.cnt - (is_sig ? out : 0u), 3u);
+    const uint32_t c0 = (is_sig | is_sign) ? sig_next : kSignSlot;
+    const uint32_t c1 = is_sig ? (uint32_t)kCtxMag
+                               : (is_mag ? (k1 < 12u ? (uint32_t)kCtxMag + k1 : kSignSlot) : c0);
+    const uint32_t q0 = ctx[c0 * 32];
+    const uint32_t q1 = ctx[c1 * 32];
+    // this bin
+    const uint32_t p0 = L.pc;
+    const uint32_t r0 = is_byp ? L.range >> 1 : (L.range >> 12) * p0;
+    const bool bit = live & (L.code >= r0);
+    const uint32_t b = bit ? 1u : 0u;
+    const uint32_t code = bit ? L.code - r0 : L.code;
+    const uint32_t range = !live ? L.range : ((bit & !is_byp) ? L.range - r0 : r0);
+    const uint32_t np0 = p0 + (uint32_t)((int)((bit ? 15u : 4096u) - p0) >> 4);
+    sts_if(live & !is_byp, ctx + L.cc * 32, np0);
+    // renormalisation, first byte (src/mc_codec.c:202)
+    const bool need = range < (1u << 24);
+    L.code = need ? __byte_perm(code, L.w, L.sel) : code;
+    L.range = need ? range << 8 : range;
+    L.sel += need ? 1u : 0u;
+    // next bin's context
+    const uint32_t ncc = bit ? c1 : c0;
+    const uint32_t nq = bit ? q1 : q0;
+    L.pc = live ? ((ncc == L.cc && !is_byp) ? np0 : nq) : L.pc;
+    L.cc = live ? ncc : L.cc;
 
-    if (sig) {
-        L.hist = (L.hist << 1) | (bit ? 1u : 0u);
-        L.cnt = L.cnt + (bit ? 1u : 0u) - ((L.hist >> 16) & 1u);
-        L.k = 0;
-        if (bit) L.st = F_MAG;
-        else advance(L, s_bend);
-    } else if (!sign) {   // F_MAG, rung k
-        L.m = L.k + 1;
-        if (!bit) L.st = F_SIGN;
-        else if (L.k == 11) { L.st = S_EGP; L.nbits = 0; L.ret = R_MAG; }
-        else L.k++;
-    } else {              // F_SIGN: the coefficient is complete
-        const uint32_t m = L.m;
-        if (put_entry(L, P, (uint32_t)s_scan[L.p] | ((bit ? 0u - m : m) << 16))) {
-            L.st = F_SIG;
-            advance(L, s_bend);
+    // significance history (the flag leaving the 16-position window drops out of cnt)
+    L.hist = is_sig ? (L.hist << 1) | b : L.hist;
+    L.cnt = is_sig ? L.cnt + b - out : L.cnt;
+    const uint32_t m = L.m;
+    L.m = is_mag ? k1 : m;
+    const bool esc = is_mag & bit & (L.k == 11);            // 12th rung set: Exp-Golomb tail
+    L.k = live ? (((is_mag | is_egp) & bit) ? k1 : 0u) : L.k;
+    L.ret = esc ? (uint32_t)R_MAG : L.ret;
+    const uint32_t nst = is_sig ? b : (is_mag ? (bit ? (esc ? (uint32_t)F_EGP : (uint32_t)F_MAG) : (uint32_t)F_SIGN)
+                                            : (is_sign ? (uint32_t)F_SIG : (uint32_t)F_EGP));
+    L.st = live ? nst : st;
+    const bool adv = is_sig ? !bit : is_sign;
+    const bool egend = is_egp & (!bit | (k1 >= kEgBase + (uint32_t)kEgCap));
+    // a sign completes the coefficient at scan position p: its entry
+    const uint32_t v = L.p | ((bit ? 0u - m : m) << 16);
+    const bool ovf = is_sign & (L.nent >= L.cap);
+    const bool store = is_sign & !ovf;
+    stg_if(store, L.ent + L.nent, v);
+    L.nent += store ? 1u : 0u;
+    const uint32_t np = L.p + (adv ? 1u : 0u);
+    L.p = np;
+    const bool event = adv & (np >= L.stop);
+    if ((L.sel == kSel0 + 4) | (L.range < (1u << 24)) | ovf | egend | event) {
+        if (L.sel == kSel0 + 4) refill(L);
+        renorm(L);
+        if (ovf && !put_entry(L, P, v)) return;   // corrupt stream: pool exhausted, block ends
+        if (egend) {
+            if (bit) { L.bad = 1; L.st = S_DONE; return; }   // prefix cap reached (corrupt stream)
+            const uint32_t nb = k1 - 1u - kEgBase;           // one-bits of the prefix
+            if (nb == 0) eg_return(L, P, 0);
+            else { L.st = S_EGS; L.rem = nb; L.acc = 0; L.k = kEgBase + nb; }
         }
+        if (event) position_event(L, ctx, s_bend);
     }
 }
 
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
-    __shared__ uint16_t s_scan[kN3];   // scan position -> raster idx
     __shared__ uint16_t s_bend[9];     // s_bend[b]: first scan position past band b
     __shared__ uint32_t s_ctx[WARPS][kCtxSlots][32];
-    for (int i = threadIdx.x; i < kN3; i += blockDim.x) {
-        const uint32_t v = P.scan[i], b = v >> 12;
-        s_scan[i] = (uint16_t)(v & 0xFFFu);
-        if (i > 0 && (P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
+    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
+        const uint32_t b = P.scan[i] >> 12;
+        if ((P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
     }
     if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
     __syncthreads();
@@ -369,34 +414,39 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
 
     // Work: the first ncoded entries of the processing order (longest payload
     // first). Each lane starts with one block; later blocks come from a shared
-    // counter as lanes finish, so long and short blocks even out.
+    // counter as lanes finish, so long and short blocks even out. A lane
+    // without a block holds a valid decoder state that the bin step passes
+    // through unchanged.
     LaneState L;
-    L.st = S_IDLE;
+    memset(&L, 0, sizeof L);
+    L.range = 0xFFFFFFFFu;
+    L.sel = kSel0;
+    L.st = S_DONE;
     L.item = -1;
-    {
-        const int first = blockIdx.x * blockDim.x + threadIdx.x;
-        if (first < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[first] : first);
-    }
+    int first = blockIdx.x * blockDim.x + threadIdx.x;
 
-    // Outer loop: block ends and slow steps of single lanes. Inner loop: two
-    // coefficient bins per live lane per round, for as long as no lane needs
-    // the outer loop (idle lanes sit it out). Every block ends after a bounded
-    // number of bins (finite scan, capped Exp-Golomb prefixes), and every lane
-    // fetches at most ncoded blocks, so both loops terminate.
+    // Outer loop: block ends and starts, and slow steps of single lanes (the
+    // other lanes take a bin meanwhile). Inner loop: two bins per live lane
+    // per round, for as long as no lane needs the outer loop. Every block ends
+    // after a bounded number of bins (finite scan, capped Exp-Golomb
+    // prefixes), and every lane fetches at most ncoded blocks, so both loops
+    // terminate.
     for (;;) {
         const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
         if (idle == 0xFFFFFFFFu) break;
-        for (;;) {
-            if (L.st <= F_SIGN) fast_step(L, P, ctx, s_scan, s_bend);
-            if (L.st <= F_SIGN) fast_step(L, P, ctx, s_scan, s_bend);
-            if (__ballot_sync(0xFFFFFFFFu, L.st > F_SIGN) != idle) break;
+        while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
+            fast_step(L, P, ctx, s_bend);
+            fast_step(L, P, ctx, s_bend);
         }
-        if (L.st > F_SIGN && L.st < S_DONE) slow_step(L, P);
+        fast_step(L, P, ctx, s_bend);
+        if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
         if (L.st == S_DONE) {
-            lane_finish(L, P);
-            L.st = S_IDLE;
-            const int nx = nlanes + (int)atomicAdd(P.status + 2, 1u);
+            if (L.item >= 0) lane_finish(L, P);
+            const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.status + 2, 1u);
+            first = -1;
+            L.item = -1;
             if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[nx] : nx);
+            else L.st = S_IDLE;
         }
     }
 }
@@ -529,7 +579,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         __syncthreads();
         int mz = 0, my = 0, mx = 0;
         for (int j = tid; j < nnz; j += 128) {
-            const uint32_t e = entry_at(P, base, cap, h.ovf, j);
+            const uint32_t e = __ldg(P.scan + (entry_at(P, base, cap, h.ovf, j) & 0xFFFu)) & 0xFFFu;
             mz = max(mz, (int)((e >> 8) & 15));
             my = max(my, (int)((e >> 4) & 15));
             mx = max(mx, (int)(e & 15));
@@ -545,7 +595,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
         for (int j = tid; j < nnz; j += 128) {
             const uint32_t e = entry_at(P, base, cap, h.ovf, j);
-            const int idx = e & 0xFFF;
+            const int idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFF;
             const int lv = (int16_t)(e >> 16);
             if (!lv) continue;
             const int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;

@@ -80,7 +80,7 @@ struct EntHdr {
 };
 static_assert(sizeof(EntHdr) == 16, "EntHdr layout");
 
-// Entry list of a block: nnz coefficient entries (idx | level<<16) followed by
+// Entry list of a block: nnz coefficient entries (scan position | level<<16) followed by
 // ncorr correction pairs (pos, wrapping delta).  The first cap entries live in
 // the arena at the block's base; later ones continue in the overflow pool.
 MCB_HD inline uint32_t entry_cap(uint32_t len) {

@@ -39,6 +39,7 @@ struct RecParams {
     const uint32_t *arena;
     const uint32_t *pool;
     const QTab *qtab;
+    const uint16_t *scan;      // scan position -> raster idx | band<<12
 };
 
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);

@@ -198,6 +198,7 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     rp.arena = ep.arena;
     rp.pool = ep.pool;
     rp.qtab = ep.qtab;
+    rp.scan = ep.scan;
     LaunchCfg cfg;
     e = cudaGetLastError();
     if (e == cudaSuccess) e = launch_entropy(ep, cfg, s);

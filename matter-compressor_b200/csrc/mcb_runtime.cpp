@@ -283,6 +283,7 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         rp.arena = B.arena.as<uint32_t>();
         rp.pool = B.pool.as<uint32_t>();
         rp.qtab = R->d_qtab;
+        rp.scan = R->d_scan;
         if (rec && !cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
     }
     return true;
