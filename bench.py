@@ -43,9 +43,10 @@ from shard import Dist, chunk_seeds, air_fraction  # noqa: E402
 CHUNK = 256 ** 3
 METRIC = "decoded GB/s per B200 at q=6 (bit-exact); p50/p99 block-request latency"
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes per decoded chunk of the entropy stage, measured with ncu on an
-# 8-chunk case and scaled per chunk (profiles/k_entropy_decode_q6.md).
-ENTROPY_DRAM_BYTES_PER_CHUNK = None
+# DRAM bytes (read + write) per decoded chunk of the entropy stage, measured
+# with ncu on a 16-chunk case and scaled per chunk
+# (profiles/k_entropy_decode_q6_16chunks.md).
+ENTROPY_DRAM_BYTES_PER_CHUNK = 16.690176e6 / 16
 
 
 def parse():

@@ -156,10 +156,12 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    auto time_cfg = [&](const LaunchCfg &c) {
-        decode_enqueue(B, c, s);   // warm
+    // one stage at a time: reconstruction reruns on the entropy output left
+    // by the entropy trials
+    auto time_cfg = [&](const LaunchCfg &c, int stage) {
+        decode_enqueue_stage(B, c, stage, s);   // warm
         cudaEventRecord(e0, s);
-        for (int r = 0; r < 2; ++r) decode_enqueue(B, c, s);
+        for (int r = 0; r < 3; ++r) decode_enqueue_stage(B, c, stage, s);
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -172,7 +174,7 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
     for (int e : ent_opts) {
         LaunchCfg c = best;
         c.ent_ctas_per_sm = e;
-        float ms = time_cfg(c);
+        float ms = time_cfg(c, 0);
         if (ms < best_ms) { best_ms = ms; best = c; }
     }
     best_ms = 1e30f;
@@ -180,7 +182,7 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
     for (int r : rec_opts) {
         LaunchCfg c = base;
         c.rec_ctas_per_sm = r;
-        float ms = time_cfg(c);
+        float ms = time_cfg(c, 1);
         if (ms < best_ms) { best_ms = ms; best = c; }
     }
     cudaEventDestroy(e0);
