@@ -161,6 +161,49 @@ void mc_b200_plan_free(mc_b200_plan *p);
 int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
                           const mc_u8 *const *vox, int vox_on_device, float q);
 
+/* Serving: block, region and chunk reads of one archive, batched continuously
+ * on the GPU behind a decoded-block cache in HBM -- the device-side analogue
+ * of the reference's mc_cache read path (src/mc_cache.h). Requests queue on
+ * submit; a worker thread admits them into a batch while the batch's output
+ * bytes stay within batch_bytes and their missing blocks find free cache
+ * slots, decodes the misses into the cache, gathers every request's blocks
+ * into its output and completes the tickets. Eviction is FIFO over slots no
+ * batch in flight is using. Results are byte-identical to
+ * mc_archive_decode_block / read_region / decode_chunk.
+ *
+ * out_on_device: request outputs are DEVICE pointers (any strides for
+ * regions); otherwise HOST pointers (dense outputs only), copied back inside
+ * the batch. The archive must not be appended to while the server is open. */
+typedef struct mc_b200_server mc_b200_server;
+enum { MC_B200_REQ_BLOCK = 0, MC_B200_REQ_REGION = 1, MC_B200_REQ_CHUNK = 2 };
+typedef struct {
+    int kind;              /* MC_B200_REQ_* */
+    int lod;
+    long z, y, x;          /* block: block coordinates; chunk: chunk coordinates; region: voxel origin */
+    long dz, dy, dx;       /* region extent in voxels (ignored otherwise) */
+    mc_u8 *out;            /* block: 4096 bytes z,y,x; chunk: 256^3 z,y,x; region: crop at out + z*sz + y*sy + x */
+    size_t sz, sy;         /* region output byte strides; 0 = dense (dy*dx, dx) */
+} mc_b200_request;
+mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t batch_bytes, int out_on_device);
+/* Returns a ticket (>= 0) or -1 for an invalid request. */
+long mc_b200_server_submit(mc_b200_server *s, const mc_b200_request *r);
+/* 1 done, 0 pending, -1 failed or unknown ticket. */
+int  mc_b200_server_poll(mc_b200_server *s, long ticket);
+/* Blocks until the ticket completes: 0 done, -1 failed. */
+int  mc_b200_server_wait(mc_b200_server *s, long ticket);
+/* Steady-clock submit and completion times of a ticket (ns); returns its state. */
+int  mc_b200_server_ticket_times(mc_b200_server *s, long ticket, uint64_t *submit_ns, uint64_t *done_ns);
+/* Trace replay: submits reqs[i] at arrival_ns[i] after the call starts (i in
+ * order), waits for all, and stores each completion time minus its arrival
+ * time in latency_ns (may be NULL). Returns 0, or -1 if any request failed. */
+int  mc_b200_server_replay(mc_b200_server *s, const mc_b200_request *reqs, const uint64_t *arrival_ns, int n,
+                           uint64_t *latency_ns);
+/* requests, batches, blocks, cache hits, misses (decoded), zero blocks,
+ * evictions, output bytes. */
+void mc_b200_server_stats(mc_b200_server *s, uint64_t out[8]);
+/* Completes every queued request, then frees the server. */
+void mc_b200_server_close(mc_b200_server *s);
+
 /* Allocation-free block decode. This entry point has no counterpart in the
  * reference; it is for callers that must not allocate memory: code running
  * inside a memory pool's or allocator's own hooks (an allocation there would

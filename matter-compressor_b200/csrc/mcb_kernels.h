@@ -10,7 +10,7 @@ namespace mcb {
 // Launch shape knobs, picked per quality by the autotuner.
 struct LaunchCfg {
     int ent_ctas_per_sm = 5;   // entropy stage: CTAs of 4 warps per SM (<= 5: 44 KB smem)
-    int rec_ctas_per_sm = 5;   // reconstruction stage: CTAs of 128 threads per SM (<= 5: 40 KB smem)
+    int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
 };
 
 struct EntParams {
@@ -43,6 +43,9 @@ struct RecParams {
 };
 
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
+// Copies decoded blocks into outputs: item.src is a dense 16^3 block (4096
+// bytes) or 0 for zeros; dst, strides and clip box as for decoding.
+cudaError_t launch_gather(const DecItem *d_items, int n, cudaStream_t s);
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStream_t s);
 

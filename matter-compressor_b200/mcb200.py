@@ -30,6 +30,13 @@ _libc = C.CDLL(None)
 _libc.free.argtypes = [C.c_void_p]
 
 
+class McRequest(C.Structure):
+    """mc_b200_request (include/matter_compressor_b200.h)."""
+    _fields_ = [("kind", C.c_int), ("lod", C.c_int), ("z", C.c_long), ("y", C.c_long), ("x", C.c_long),
+                ("dz", C.c_long), ("dy", C.c_long), ("dx", C.c_long), ("out", C.c_void_p),
+                ("sz", C.c_size_t), ("sy", C.c_size_t)]
+
+
 def _ptr(a):
     return C.c_void_p(a.ctypes.data)
 
@@ -105,6 +112,14 @@ class McLib:
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
                 "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
+                "mc_b200_server_open": (vp, [vp, sz, sz, i]),
+                "mc_b200_server_submit": (lg, [vp, C.POINTER(McRequest)]),
+                "mc_b200_server_poll": (i, [vp, lg]),
+                "mc_b200_server_wait": (i, [vp, lg]),
+                "mc_b200_server_ticket_times": (i, [vp, lg, C.POINTER(u64), C.POINTER(u64)]),
+                "mc_b200_server_replay": (i, [vp, C.POINTER(McRequest), vp, i, vp]),
+                "mc_b200_server_stats": (None, [vp, vp]),
+                "mc_b200_server_close": (None, [vp]),
             })
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -330,6 +345,65 @@ class Plan:
         if self.p:
             self.lib.L.mc_b200_plan_free(self.p)
             self.p = None
+
+
+REQ_BLOCK, REQ_REGION, REQ_CHUNK = 0, 1, 2
+
+
+class Server:
+    """mc_b200_server: continuous batching of block / region / chunk reads
+    behind an HBM decoded-block cache."""
+
+    STATS = ("requests", "batches", "blocks", "hits", "misses", "zero_blocks", "evictions", "bytes")
+
+    def __init__(self, archive, cache_bytes, batch_bytes=0, on_device=True):
+        self.lib = archive.lib
+        self.s = self.lib.L.mc_b200_server_open(archive.a, cache_bytes, batch_bytes, 1 if on_device else 0)
+        if not self.s:
+            self.lib.check()
+            raise RuntimeError("mc_b200_server_open failed")
+
+    @staticmethod
+    def request(kind, lod, z, y, x, out, dz=0, dy=0, dx=0, sz=0, sy=0):
+        return McRequest(kind, lod, z, y, x, dz, dy, dx, out, sz, sy)
+
+    def submit(self, req):
+        return self.lib.L.mc_b200_server_submit(self.s, C.byref(req))
+
+    def wait(self, ticket):
+        return self.lib.L.mc_b200_server_wait(self.s, ticket)
+
+    def poll(self, ticket):
+        return self.lib.L.mc_b200_server_poll(self.s, ticket)
+
+    def times(self, ticket):
+        a, b = C.c_uint64(), C.c_uint64()
+        st = self.lib.L.mc_b200_server_ticket_times(self.s, ticket, C.byref(a), C.byref(b))
+        return st, a.value, b.value
+
+    def replay(self, reqs, arrival_ns):
+        n = len(reqs)
+        arr = (McRequest * n)(*reqs)
+        t = np.ascontiguousarray(arrival_ns, np.uint64)
+        lat = np.zeros(n, np.uint64)
+        rc = self.lib.L.mc_b200_server_replay(self.s, arr, _ptr(t), n, _ptr(lat))
+        return rc, lat
+
+    def stats(self):
+        out = np.zeros(8, np.uint64)
+        self.lib.L.mc_b200_server_stats(self.s, _ptr(out))
+        return dict(zip(self.STATS, (int(v) for v in out)))
+
+    def close(self):
+        if self.s:
+            self.lib.L.mc_b200_server_close(self.s)
+            self.s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def decode_chunk_blobs(lib, blobs, out=None):
