@@ -22,6 +22,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <memory>
 #include <atomic>
 #include <mutex>
 #include <vector>
@@ -190,9 +191,14 @@ uint64_t resolve_chunk(const uint8_t *arc, uint64_t root, int cz, int cy, int cx
 
 namespace mcb {
 // keyed by (archive base, chunk offset, stored hash): a reused offset with new
-// content never serves a stale index
+// content never serves a stale index. Each thread keeps the indexes of its 32
+// most recent chunks (direct-mapped by offset), so block walks that alternate
+// between neighbouring chunks (regions across chunk borders) reuse them.
 const ChunkIndex &chunk_index(const uint8_t *arc, uint64_t co) {
-    static thread_local ChunkIndex ix;
+    constexpr int kWays = 32;
+    static thread_local std::unique_ptr<ChunkIndex[]> cache;
+    if (!cache) cache.reset(new ChunkIndex[kWays]);
+    ChunkIndex &ix = cache[(co * 0x9E3779B97F4A7C15ull) >> 59];
     uint64_t tag = rd64(arc + co + 4);
     if (ix.arc == arc && ix.chunk_off == co && ix.tag == tag) return ix;
     uint16_t fml;

@@ -43,9 +43,28 @@ struct RecParams {
 };
 
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
-// Copies decoded blocks into outputs: item.src is a dense 16^3 block (4096
-// bytes) or 0 for zeros; dst, strides and clip box as for decoding.
-cudaError_t launch_gather(const DecItem *d_items, int n, cudaStream_t s);
+// ---- serving ----
+// One chunk's share of a request: a box of blocks, the request's voxel clip in
+// chunk-local coordinates, and where chunk-local voxel (0,0,0) maps in the output.
+constexpr uint32_t kNoTable = 0xFFFFFFFFu;    // chunk absent or all air: zeros
+constexpr uint32_t kZeroSlot = 0xFFFFFFFEu;   // table entry of an absent block
+constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;  // table entry not resolved yet
+struct GatherItem {
+    uint64_t dst;              // output address of chunk-local voxel (0,0,0)
+    int64_t sz, sy;            // output byte strides
+    uint32_t table;            // slot table of the chunk, or kNoTable
+    uint32_t first;            // flattened index of the item's first block
+    uint16_t box_lo, box_hi;   // block box (z<<8|y<<4|x), inclusive
+    uint8_t lo[3], hi[3];      // voxel clip (z, y, x), chunk-local, inclusive
+    uint8_t pad[2];
+};
+static_assert(sizeof(GatherItem) == 48, "GatherItem layout");
+// tables[u.x] = u.y for each update
+cudaError_t launch_table_update(const uint2 *d_upd, int n, uint32_t *d_tables, cudaStream_t s);
+// Copies every block of every item from the cache (slot s at cache + s*4096,
+// dense z,y,x) into the outputs; nblocks = sum of the items' block counts.
+cudaError_t launch_gather_boxes(const GatherItem *d_items, int nitems, uint32_t nblocks, const uint32_t *d_tables,
+                                const uint8_t *d_cache, cudaStream_t s);
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStream_t s);
 

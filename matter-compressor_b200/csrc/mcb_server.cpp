@@ -48,7 +48,6 @@ using namespace mcb;
 namespace {
 
 constexpr size_t kChunkBytes = (size_t)256 * 256 * 256;
-constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 
 uint64_t now_ns() {
     return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -60,14 +59,28 @@ struct Ticket {
     uint64_t t_submit = 0, t_done = 0;
 };
 
+// Cache bookkeeping of one chunk blob (keyed by its archive offset): the
+// cache slot of each of its blocks, mirrored in a device table the gather
+// reads. kEmptySlot: not resolved yet; kZeroSlot: an absent block.
+struct ChunkRes {
+    uint64_t co = 0;
+    uint32_t table = 0;
+    uint32_t resolved = 0, resident = 0, pins = 0;
+    uint64_t pin_seq = 0, last_use = 0;
+    int qslot = -1;
+    uint32_t slot[kGrid3];
+};
+
 struct SrvBatch {
     DecodeBatch dec;                          // the batch's cache misses
-    std::vector<DecItem> gather;              // every requested block -> its output
-    HostBuf h_gather;
-    DevBuf d_gather, staging;                 // staging: outputs of host-memory requests
     std::vector<DecItem> miss;                // blocks to decode into their cache slots
+    std::vector<GatherItem> gather;           // every request's chunk pieces
+    std::vector<uint2> upd;                   // slot-table writes
+    uint32_t nblocks = 0;
+    HostBuf h_gather, h_upd;
+    DevBuf d_gather, d_upd, staging;          // staging: outputs of host-memory requests
     std::vector<long> tickets;
-    std::vector<uint32_t> pins;               // cache slots the batch reads or fills
+    std::vector<ChunkRes *> pins;             // chunks the batch reads
     struct D2H { void *dst; size_t off, bytes; };
     std::vector<D2H> d2h;
     size_t staged = 0;                        // staging bytes (host outputs)
@@ -82,12 +95,19 @@ struct mc_b200_server {
     mc_archive *a = nullptr;
     bool dev_out = true;
     size_t batch_bytes = 0;
-    // decoded-block cache
+    // decoded-block cache: slots of 4096 bytes, FIFO hand
     uint8_t *d_cache = nullptr;
-    uint32_t nslots = 0, hand = 0, npinned = 0;
-    std::unordered_map<uint64_t, uint32_t> map;   // (chunk offset << 12 | block) -> slot
-    std::vector<uint64_t> slot_key;
-    std::vector<uint32_t> slot_pin;
+    uint32_t nslots = 0, hand = 0, pinned_slots = 0;
+    std::vector<ChunkRes *> slot_owner;
+    std::vector<uint16_t> slot_block;
+    // per-chunk slot tables (device) and their owners
+    uint32_t *d_tables = nullptr;
+    uint32_t ntables = 0;
+    std::vector<ChunkRes *> table_owner;
+    std::vector<uint32_t> free_tables;
+    std::unordered_map<uint64_t, ChunkRes *> chunks;
+    uint64_t use_clock = 0;
+    std::vector<uint2> pending_upd;   // table writes of a formed batch that admitted nothing
     // requests
     std::mutex mu;
     std::condition_variable cv;
@@ -114,18 +134,16 @@ size_t out_bytes(const mc_b200_request &r) {
     }
 }
 
-// One block of a request: where it comes from and where it goes.
-struct Need {
-    uint64_t key;         // 0: zeros (absent block, chunk or out of the volume)
-    uint64_t pay_off;     // payload offset in the archive
-    uint32_t len;
-    uint16_t qslot;
-    DecItem g;            // gather item (src filled in once the slot is known)
+// One chunk's share of a request, before cache resolution.
+struct Piece {
+    long cz, cy, cx;
+    int lo[3], hi[3];   // voxel clip, chunk-local, inclusive
+    GatherItem g;
 };
 
-// The blocks of one request, in output coordinates (the same block walk as the
-// region read, src/mc_archive.c:984-1042).
-bool enumerate(mc_b200_server *S, const mc_b200_request &r, uint8_t *out, std::vector<Need> &need) {
+// The chunk pieces of one request, in output coordinates (the block walk of
+// the region read, src/mc_archive.c:984-1042, grouped by chunk).
+void pieces_of(const mc_b200_request &r, uint8_t *out, std::vector<Piece> &ps) {
     long z0, y0, x0, dz, dy, dx;
     int64_t sz, sy;
     if (r.kind == MC_B200_REQ_BLOCK) {
@@ -137,147 +155,214 @@ bool enumerate(mc_b200_server *S, const mc_b200_request &r, uint8_t *out, std::v
         sz = r.sz ? (int64_t)r.sz : (int64_t)(dy * dx);
         sy = r.sy ? (int64_t)r.sy : (int64_t)dx;
     }
-    mc_archive *a = S->a;
-    const uint64_t cur = a->cursor.load(std::memory_order_acquire);
-    const long bz0 = z0 >> 4, by0 = y0 >> 4, bx0 = x0 >> 4;
-    const long nbz = ((z0 + dz + 15) >> 4) - bz0, nby = ((y0 + dy + 15) >> 4) - by0, nbx = ((x0 + dx + 15) >> 4) - bx0;
-    long last_cz = -1, last_cy = -1, last_cx = -1;
-    uint64_t co = 0;
-    int slot = 0;
-    for (long w = 0; w < nbz * nby * nbx; ++w) {
-        const long bz = bz0 + w / (nby * nbx), by = by0 + (w / nbx) % nby, bx = bx0 + w % nbx;
-        const long gz = bz * 16, gy = by * 16, gx = bx * 16;
-        const long iz0 = std::max(gz, z0), iz1 = std::min(gz + 16, z0 + dz);
-        const long iy0 = std::max(gy, y0), iy1 = std::min(gy + 16, y0 + dy);
-        const long ix0 = std::max(gx, x0), ix1 = std::min(gx + 16, x0 + dx);
-        if (iz0 >= iz1 || iy0 >= iy1 || ix0 >= ix1) continue;
-        const long cz = bz >> 4, cy = by >> 4, cx = bx >> 4;
-        if (cz != last_cz || cy != last_cy || cx != last_cx) {
-            co = mc_archive_chunk_offset(a, r.lod, (int)cz, (int)cy, (int)cx);
-            last_cz = cz; last_cy = cy; last_cx = cx;
-            if (co > kSlotZero) {
-                slot = qslot(sanitize_q(chunk_q(a, co)));
-                if (slot < 0) return false;
+    const long c0[3] = {z0 >> 8, y0 >> 8, x0 >> 8};
+    const long c1[3] = {(z0 + dz - 1) >> 8, (y0 + dy - 1) >> 8, (x0 + dx - 1) >> 8};
+    const long org[3] = {z0, y0, x0}, ext[3] = {dz, dy, dx};
+    for (long cz = c0[0]; cz <= c1[0]; ++cz)
+        for (long cy = c0[1]; cy <= c1[1]; ++cy)
+            for (long cx = c0[2]; cx <= c1[2]; ++cx) {
+                Piece p;
+                memset(&p, 0, sizeof p);
+                p.cz = cz; p.cy = cy; p.cx = cx;
+                const long cc[3] = {cz, cy, cx};
+                for (int a = 0; a < 3; ++a) {
+                    p.lo[a] = (int)(std::max(org[a], cc[a] * 256) - cc[a] * 256);
+                    p.hi[a] = (int)(std::min(org[a] + ext[a], cc[a] * 256 + 256) - 1 - cc[a] * 256);
+                }
+                p.g.dst = (uint64_t)(uintptr_t)(out + (cz * 256 - z0) * sz + (cy * 256 - y0) * sy + (cx * 256 - x0));
+                p.g.sz = sz;
+                p.g.sy = sy;
+                p.g.table = kNoTable;
+                p.g.box_lo = (uint16_t)((p.lo[0] >> 4) << 8 | (p.lo[1] >> 4) << 4 | (p.lo[2] >> 4));
+                p.g.box_hi = (uint16_t)((p.hi[0] >> 4) << 8 | (p.hi[1] >> 4) << 4 | (p.hi[2] >> 4));
+                for (int a = 0; a < 3; ++a) { p.g.lo[a] = (uint8_t)p.lo[a]; p.g.hi[a] = (uint8_t)p.hi[a]; }
+                ps.push_back(p);
             }
-        }
-        Need n;
-        memset(&n, 0, sizeof n);
-        if (co > kSlotZero) {
-            const ChunkIndex &ix = chunk_index(a->base, co);
-            const int bi = (int)(((bz & 15) * 16 + (by & 15)) * 16 + (bx & 15));
-            const uint64_t off = ix.off[bi];
-            if (off && off + ix.len[bi] <= cur) {
-                n.key = (co << 12) | (uint64_t)bi;
-                n.pay_off = off;
-                n.len = ix.len[bi];
-                n.qslot = (uint16_t)slot;
-            }
-        }
-        n.g.dst = (uint64_t)(uintptr_t)(out + (gz - z0) * sz + (gy - y0) * sy + (gx - x0));
-        n.g.sz = sz;
-        n.g.sy = sy;
-        n.g.clip_lo = (uint16_t)(((iz0 - gz) << 8) | ((iy0 - gy) << 4) | (ix0 - gx));
-        n.g.clip_hi = (uint16_t)(((iz1 - 1 - gz) << 8) | ((iy1 - 1 - gy) << 4) | (ix1 - 1 - gx));
-        need.push_back(n);
-    }
-    return true;
 }
 
-// Next unpinned slot in FIFO order (the caller has checked that one exists);
-// its old block, if any, leaves the cache.
+uint32_t box_blocks(const GatherItem &g) {
+    return (uint32_t)(((g.box_hi >> 8) - (g.box_lo >> 8) + 1) * (((g.box_hi >> 4) & 15) - ((g.box_lo >> 4) & 15) + 1) *
+                      ((g.box_hi & 15) - (g.box_lo & 15) + 1));
+}
+
+void pin_chunk(mc_b200_server *S, SrvBatch &B, ChunkRes *c) {
+    if (c->pin_seq == B.seq) return;
+    c->pin_seq = B.seq;
+    if (c->pins++ == 0) S->pinned_slots += c->resident;
+    B.pins.push_back(c);
+}
+
+void unpin_chunk(mc_b200_server *S, ChunkRes *c) {
+    if (--c->pins == 0) S->pinned_slots -= c->resident;
+}
+
+void release_slot(mc_b200_server *S, uint32_t s) {
+    ChunkRes *o = S->slot_owner[s];
+    if (!o) return;
+    const uint32_t bi = S->slot_block[s];
+    // the device table keeps the stale number: the gather reads an entry only
+    // after the block was resolved again, which rewrites it
+    o->slot[bi] = kEmptySlot;
+    o->resolved--;
+    o->resident--;
+    S->slot_owner[s] = nullptr;
+    S->st_evict++;
+}
+
+// Next slot in FIFO order whose chunk no batch holds; the caller has checked
+// that one exists.
 uint32_t take_slot(mc_b200_server *S) {
     for (;;) {
         const uint32_t s = S->hand;
         S->hand = S->hand + 1 == S->nslots ? 0 : S->hand + 1;
-        if (S->slot_pin[s]) continue;
-        if (S->slot_key[s]) {
-            S->map.erase(S->slot_key[s]);
-            S->slot_key[s] = 0;
-            S->st_evict++;
-        }
+        ChunkRes *o = S->slot_owner[s];
+        if (o && o->pins) continue;
+        release_slot(S, s);
         return s;
     }
 }
 
-void pin(mc_b200_server *S, SrvBatch &B, uint32_t s) {
-    if (S->slot_pin[s]++ == 0) S->npinned++;
-    B.pins.push_back(s);
+// The bookkeeping of chunk co, created on first use; when every slot table is
+// taken, the least recently used chunk no batch holds gives up its table and
+// its slots. Null if every table belongs to a held chunk.
+ChunkRes *chunk_res(mc_b200_server *S, uint64_t co) {
+    auto it = S->chunks.find(co);
+    if (it != S->chunks.end()) return it->second;
+    if (S->free_tables.empty()) {
+        ChunkRes *victim = nullptr;
+        for (auto &kv : S->chunks)
+            if (!kv.second->pins && (!victim || kv.second->last_use < victim->last_use)) victim = kv.second;
+        if (!victim) return nullptr;
+        for (uint32_t bi = 0; bi < (uint32_t)kGrid3; ++bi) {
+            const uint32_t s = victim->slot[bi];
+            if (s < kZeroSlot) { S->slot_owner[s] = nullptr; S->st_evict++; }
+        }
+        S->chunks.erase(victim->co);
+        S->table_owner[victim->table] = nullptr;
+        S->free_tables.push_back(victim->table);
+        delete victim;
+    }
+    ChunkRes *c = new ChunkRes();
+    c->co = co;
+    c->table = S->free_tables.back();
+    S->free_tables.pop_back();
+    // a reused table may hold another chunk's slots on the device; each entry is
+    // rewritten when its block is resolved, before any gather reads it, and
+    // every entry is written at most once per batch
+    for (uint32_t bi = 0; bi < (uint32_t)kGrid3; ++bi) c->slot[bi] = kEmptySlot;
+    S->table_owner[c->table] = c;
+    S->chunks[co] = c;
+    return c;
 }
 
-// Forms a batch from the queue head (caller holds the lock). Device-side
-// addresses of the archive mirror come from dbase.
-// Allocates nothing on the device: buffers grow in launch(), outside the lock
-// that the completion callback takes.
+// Forms a batch from the queue head (caller holds the lock). Allocates nothing
+// on the device: buffers grow in launch(), outside the lock that the completion
+// callback takes.
 void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
     B.gather.clear();
+    B.miss.clear();
+    B.upd.swap(S->pending_upd);   // writes left over from an empty batch go first
+    S->pending_upd.clear();
     B.tickets.clear();
     B.pins.clear();
     B.d2h.clear();
-    B.miss.clear();
-    std::vector<DecItem> &miss = B.miss;
-    std::vector<Need> need;
+    B.nblocks = 0;
+    B.seq = ++S->seq;
+    mc_archive *a = S->a;
+    const uint64_t cur = a->cursor.load(std::memory_order_acquire);
+    std::vector<Piece> ps;
+    std::vector<std::pair<ChunkRes *, uint32_t>> misses;   // (chunk, block) to decode
     size_t bytes = 0, staged = 0;
     while (!S->queue_req.empty()) {
         const mc_b200_request r = S->queue_req.front();
         const long t = S->queue_tk.front();
         const size_t nb = out_bytes(r);
         if (!B.tickets.empty() && bytes + nb > S->batch_bytes) break;
-        // host outputs land in the batch's staging buffer first
-        uint8_t *out = S->dev_out ? r.out : reinterpret_cast<uint8_t *>(staged);   // offset until the buffer exists
-        need.clear();
-        if (!enumerate(S, r, out, need)) {
+        // host outputs land in the batch's staging buffer (offsets until launch)
+        uint8_t *out = S->dev_out ? r.out : reinterpret_cast<uint8_t *>(staged);
+        ps.clear();
+        pieces_of(r, out, ps);
+        // resolve each piece's chunk; count the blocks that need a cache slot
+        misses.clear();
+        bool fail = false, no_table = false;
+        uint64_t zeros = 0;
+        for (auto &p : ps) {
+            const uint64_t co = mc_archive_chunk_offset(a, r.lod, (int)p.cz, (int)p.cy, (int)p.cx);
+            if (co <= kSlotZero) { zeros += box_blocks(p.g); continue; }   // absent or all air: zeros
+            ChunkRes *c = chunk_res(S, co);
+            if (!c) { no_table = true; break; }
+            if (c->qslot < 0) {
+                c->qslot = qslot(sanitize_q(chunk_q(a, co)));
+                if (c->qslot < 0) { fail = true; break; }
+            }
+            pin_chunk(S, B, c);   // keeps the chunk's table and slots while the batch forms
+            c->last_use = ++S->use_clock;
+            p.g.table = c->table;
+            if (c->resolved == (uint32_t)kGrid3) continue;
+            const ChunkIndex &ix = chunk_index(a->base, co);
+            for (int bz = p.lo[0] >> 4; bz <= p.hi[0] >> 4; ++bz)
+                for (int by = p.lo[1] >> 4; by <= p.hi[1] >> 4; ++by)
+                    for (int bx = p.lo[2] >> 4; bx <= p.hi[2] >> 4; ++bx) {
+                        const uint32_t bi = (uint32_t)(bz << 8 | by << 4 | bx);
+                        if (c->slot[bi] != kEmptySlot) continue;
+                        const uint64_t off = ix.off[bi];
+                        if (!off || off + ix.len[bi] > cur) {   // absent block: zeros
+                            c->slot[bi] = kZeroSlot;
+                            c->resolved++;
+                            zeros++;
+                            B.upd.push_back(make_uint2(c->table * kGrid3 + bi, kZeroSlot));
+                        } else {
+                            misses.emplace_back(c, bi);
+                        }
+                    }
+        }
+        if (fail || misses.size() > S->nslots) {   // cannot be served
             S->tickets[t].state = -1;
             S->queue_req.pop_front();
             S->queue_tk.pop_front();
             continue;
         }
-        // admission: every missing block needs a free (unpinned) cache slot
-        uint32_t misses = 0;
-        for (auto &n : need)
-            if (n.key && !S->map.count(n.key)) misses++;
-        if (misses > S->nslots - S->npinned) {
-            if (misses > S->nslots) {   // larger than the whole cache: refused
-                S->tickets[t].state = -1;
-                S->queue_req.pop_front();
-                S->queue_tk.pop_front();
-                continue;
-            }
+        if (no_table || misses.size() > S->nslots - S->pinned_slots) {
             if (B.tickets.empty()) S->head_blocked = true;   // wait until a batch in flight retires
             break;
         }
-        for (auto &n : need) {
-            S->st_blocks++;
-            if (!n.key) {
-                n.g.src = 0;
-                S->st_zero++;
-            } else {
-                auto it = S->map.find(n.key);
-                uint32_t s;
-                if (it != S->map.end()) {
-                    s = it->second;
-                    S->st_hits++;
-                } else {
-                    s = take_slot(S);
-                    S->map[n.key] = s;
-                    S->slot_key[s] = n.key;
-                    DecItem d;
-                    memset(&d, 0, sizeof d);
-                    d.src = (uint64_t)(uintptr_t)(dbase + n.pay_off);
-                    d.len = n.len;
-                    d.dst = (uint64_t)(uintptr_t)(S->d_cache + (size_t)s * kN3);
-                    d.sz = 256;
-                    d.sy = 16;
-                    d.qslot = n.qslot;
-                    d.clip_lo = kClipFullLo;
-                    d.clip_hi = kClipFullHi;
-                    miss.push_back(d);
-                    S->st_miss++;
-                }
-                pin(S, B, s);
-                n.g.src = (uint64_t)(uintptr_t)(S->d_cache + (size_t)s * kN3);
-            }
-            B.gather.push_back(n.g);
+        for (auto &m : misses) {
+            ChunkRes *c = m.first;
+            const uint32_t bi = m.second;
+            if (c->slot[bi] != kEmptySlot) continue;   // the same block twice in one request
+            const uint32_t s = take_slot(S);
+            c->slot[bi] = s;
+            c->resolved++;
+            c->resident++;
+            S->pinned_slots++;   // c is pinned by this batch
+            S->slot_owner[s] = c;
+            S->slot_block[s] = (uint16_t)bi;
+            B.upd.push_back(make_uint2(c->table * kGrid3 + bi, s));
+            const ChunkIndex &ix = chunk_index(a->base, c->co);
+            DecItem d;
+            memset(&d, 0, sizeof d);
+            d.src = (uint64_t)(uintptr_t)(dbase + ix.off[bi]);
+            d.len = ix.len[bi];
+            d.dst = (uint64_t)(uintptr_t)(S->d_cache + (size_t)s * kN3);
+            d.sz = 256;
+            d.sy = 16;
+            d.qslot = (uint16_t)c->qslot;
+            d.clip_lo = kClipFullLo;
+            d.clip_hi = kClipFullHi;
+            B.miss.push_back(d);
         }
+        for (auto &p : ps) {
+            p.g.first = B.nblocks;
+            const uint32_t n = box_blocks(p.g);
+            B.nblocks += n;
+            S->st_blocks += n;
+            B.gather.push_back(p.g);
+        }
+        uint64_t nblk = 0;
+        for (auto &p : ps) nblk += box_blocks(p.g);
+        S->st_miss += misses.size();
+        S->st_zero += zeros;
+        S->st_hits += nblk - zeros - misses.size();
         if (!S->dev_out) {
             B.d2h.push_back({r.out, staged, nb});
             staged += (nb + 255) & ~(size_t)255;
@@ -286,6 +371,12 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
         B.tickets.push_back(t);
         S->queue_req.pop_front();
         S->queue_tk.pop_front();
+    }
+    if (B.tickets.empty()) {   // nothing admitted: let go of the chunks pinned while trying
+        for (ChunkRes *c : B.pins) unpin_chunk(S, c);
+        B.pins.clear();
+        S->pending_upd.swap(B.upd);   // the device tables still need these writes
+        B.upd.clear();
     }
     B.staged = staged;
     if (!B.tickets.empty()) S->st_batches++;
@@ -306,6 +397,14 @@ void CUDART_CB on_done(void *p) {
 // host copies, completion callback.
 bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
     cudaStream_t s = L.stream;
+    const size_t nu = B.upd.size();
+    if (nu) {
+        if (!B.h_upd.ensure(sizeof(uint2) * nu) || !B.d_upd.ensure(sizeof(uint2) * nu)) return false;
+        memcpy(B.h_upd.p, B.upd.data(), sizeof(uint2) * nu);
+        if (!cuda_ok(cudaMemcpyAsync(B.d_upd.p, B.h_upd.p, sizeof(uint2) * nu, cudaMemcpyHostToDevice, s), "H2D") ||
+            !cuda_ok(launch_table_update(B.d_upd.as<uint2>(), (int)nu, S->d_tables, s), "table update"))
+            return false;
+    }
     const int nmiss = (int)B.miss.size();
     if (nmiss) {
         if (!B.dec.h_items.ensure(sizeof(DecItem) * nmiss)) return false;
@@ -318,11 +417,12 @@ bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
     }
     const size_t ng = B.gather.size();
     if (ng) {
-        if (!B.h_gather.ensure(sizeof(DecItem) * ng) || !B.d_gather.ensure(sizeof(DecItem) * ng)) return false;
-        memcpy(B.h_gather.p, B.gather.data(), sizeof(DecItem) * ng);
-        if (!cuda_ok(cudaMemcpyAsync(B.d_gather.p, B.h_gather.p, sizeof(DecItem) * ng, cudaMemcpyHostToDevice, s),
+        if (!B.h_gather.ensure(sizeof(GatherItem) * ng) || !B.d_gather.ensure(sizeof(GatherItem) * ng)) return false;
+        memcpy(B.h_gather.p, B.gather.data(), sizeof(GatherItem) * ng);
+        if (!cuda_ok(cudaMemcpyAsync(B.d_gather.p, B.h_gather.p, sizeof(GatherItem) * ng, cudaMemcpyHostToDevice, s),
                      "H2D gather") ||
-            !cuda_ok(launch_gather(B.d_gather.as<DecItem>(), (int)ng, s), "gather launch"))
+            !cuda_ok(launch_gather_boxes(B.d_gather.as<GatherItem>(), (int)ng, B.nblocks, S->d_tables, S->d_cache, s),
+                     "gather launch"))
             return false;
     }
     for (auto &c : B.d2h)
@@ -334,8 +434,7 @@ bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
 }
 
 void retire(mc_b200_server *S, SrvBatch &B) {   // caller holds the lock
-    for (uint32_t s : B.pins)
-        if (--S->slot_pin[s] == 0) S->npinned--;
+    for (ChunkRes *c : B.pins) unpin_chunk(S, c);
     for (long t : B.tickets)
         if (S->tickets[t].state == 0) S->tickets[t].state = 1;
     B.pins.clear();
@@ -390,7 +489,6 @@ void worker_main(mc_b200_server *S) {
         if (fb->tickets.empty()) { S->cv.notify_all(); continue; }
         fb->busy = true;
         fb->gpu_done = false;
-        fb->seq = ++S->seq;
         lk.unlock();
         const bool ok = launch(S, *fb, *L);
         lk.lock();
@@ -420,9 +518,17 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
     S->batch_bytes = batch_bytes ? batch_bytes : ((size_t)256 << 20);
     S->nslots = (uint32_t)std::min<size_t>(cache_bytes / kN3, 0xFFFFFFF0u);
     if (!cuda_ok(cudaMalloc(&S->d_cache, (size_t)S->nslots * kN3), "cache alloc")) { delete S; return nullptr; }
-    S->slot_key.assign(S->nslots, 0);
-    S->slot_pin.assign(S->nslots, 0);
-    S->map.reserve(std::min<size_t>(S->nslots, 1u << 22));
+    S->slot_owner.assign(S->nslots, nullptr);
+    S->slot_block.assign(S->nslots, 0);
+    // slot tables: room for every chunk the cache could hold a block of, within reason
+    S->ntables = (uint32_t)std::min<size_t>(std::max<size_t>(S->nslots, 1024), 16384);
+    if (!cuda_ok(cudaMalloc(&S->d_tables, (size_t)S->ntables * kGrid3 * 4), "table alloc")) {
+        cudaFree(S->d_cache);
+        delete S;
+        return nullptr;
+    }
+    S->table_owner.assign(S->ntables, nullptr);
+    for (uint32_t t = S->ntables; t-- > 0;) S->free_tables.push_back(t);
     S->worker = std::thread(worker_main, S);
     return S;
 }
@@ -513,6 +619,8 @@ void mc_b200_server_close(mc_b200_server *S) {
     if (S->worker.joinable()) S->worker.join();
     cudaDeviceSynchronize();
     if (S->d_cache) cudaFree(S->d_cache);
+    if (S->d_tables) cudaFree(S->d_tables);
+    for (auto &kv : S->chunks) delete kv.second;
     delete S;
 }
 
