@@ -110,7 +110,8 @@ struct mc_b200_server {
     std::vector<uint2> pending_upd;   // table writes of a formed batch that admitted nothing
     // requests
     std::mutex mu;
-    std::condition_variable cv;
+    std::condition_variable cv;        // the worker: new requests, finished batches, close
+    std::condition_variable cv_done;   // callers waiting for tickets
     std::deque<mc_b200_request> queue_req;
     std::deque<long> queue_tk;
     std::deque<Ticket> tickets;
@@ -390,7 +391,7 @@ void CUDART_CB on_done(void *p) {
     std::lock_guard<std::mutex> g(B->srv->mu);
     for (long k : B->tickets) B->srv->tickets[k].t_done = t;
     B->gpu_done = true;
-    B->srv->cv.notify_all();
+    B->srv->cv.notify_one();
 }
 
 // Enqueues a formed batch on the stream: misses into their slots, gather,
@@ -441,7 +442,7 @@ void retire(mc_b200_server *S, SrvBatch &B) {   // caller holds the lock
     B.busy = false;
     B.gpu_done = false;
     S->head_blocked = false;
-    S->cv.notify_all();
+    S->cv_done.notify_all();
 }
 
 void worker_main(mc_b200_server *S) {
@@ -450,7 +451,7 @@ void worker_main(mc_b200_server *S) {
     if (!L) {   // no usable device: refuse everything
         S->stop = true;
         while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-        S->cv.notify_all();
+        S->cv_done.notify_all();
         return;
     }
     for (;;) {
@@ -482,11 +483,11 @@ void worker_main(mc_b200_server *S) {
         lk.lock();
         if (!dbase) {
             while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-            S->cv.notify_all();
+            S->cv_done.notify_all();
             continue;
         }
         form(S, *fb, dbase);
-        if (fb->tickets.empty()) { S->cv.notify_all(); continue; }
+        if (fb->tickets.empty()) { S->cv_done.notify_all(); continue; }   // refused requests
         fb->busy = true;
         fb->gpu_done = false;
         lk.unlock();
@@ -501,7 +502,7 @@ void worker_main(mc_b200_server *S) {
     }
     // fail whatever is still queued
     while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-    S->cv.notify_all();
+    S->cv_done.notify_all();
 }
 
 }  // namespace
@@ -549,7 +550,7 @@ long mc_b200_server_submit(mc_b200_server *S, const mc_b200_request *r) {
     S->tickets.back().t_submit = now_ns();
     S->queue_req.push_back(*r);
     S->queue_tk.push_back(t);
-    S->cv.notify_all();
+    S->cv.notify_one();
     return t;
 }
 
@@ -564,7 +565,7 @@ int mc_b200_server_wait(mc_b200_server *S, long t) {
     if (!S || t < 0) return -1;
     std::unique_lock<std::mutex> lk(S->mu);
     if ((size_t)t >= S->tickets.size()) return -1;
-    S->cv.wait(lk, [&] { return S->tickets[t].state != 0; });
+    S->cv_done.wait(lk, [&] { return S->tickets[t].state != 0; });
     return S->tickets[t].state == 1 ? 0 : -1;
 }
 
@@ -614,7 +615,7 @@ void mc_b200_server_close(mc_b200_server *S) {
     {
         std::lock_guard<std::mutex> g(S->mu);
         S->stop = true;
-        S->cv.notify_all();
+        S->cv.notify_one();
     }
     if (S->worker.joinable()) S->worker.join();
     cudaDeviceSynchronize();
