@@ -436,6 +436,7 @@ def run_b200(args, d):
     out = torch.empty(args.chunks * CHUNK, dtype=torch.uint8, device=dev)
     plan = a.plan_chunks(offs, out.data_ptr())
     launches_per_step, blocks, payload = plan.info()
+    plan_cfg = plan.config()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     s = torch.cuda.current_stream()
     for w in range(args.warmup):
@@ -546,7 +547,7 @@ def run_b200(args, d):
                      "step_frac": round(value / d.world / peak, 4)},
         "latency": {"api": "mc_archive_decode_block (plain per-call drop-in, host buffer)",
                     "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[int(len(lat) * 0.99) - 1], 4)},
-        "blocks_per_step": blocks, "payload_bytes_per_step": payload,
+        "blocks_per_step": blocks, "payload_bytes_per_step": payload, "launch_config": plan_cfg,
         "clocks": clk,
         "cpu_baseline": cpu,
     }

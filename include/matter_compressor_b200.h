@@ -152,6 +152,9 @@ int  mc_b200_plan_launch(mc_b200_plan *p, void *stream);
 int  mc_b200_plan_launch_stage(mc_b200_plan *p, int stage, void *stream);
 /* Kernel launches per replay, blocks decoded, and total payload bytes. */
 void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes);
+/* The launch shape the plan's autotuner chose: entropy CTAs per SM,
+ * reconstruction CTAs per SM, and 1 if the longest blocks run on a second stream. */
+void mc_b200_plan_config(const mc_b200_plan *p, int out[3]);
 void mc_b200_plan_free(mc_b200_plan *p);
 
 /* Batched append: encode n chunks (chunk i's 256^3 voxels at HOST vox[i], or

@@ -153,37 +153,65 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
         if (it != g_tuned.end()) return it->second;
     }
     LaunchCfg best;
+    best.split = false;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    // one stage at a time: reconstruction reruns on the entropy output left
-    // by the entropy trials
+    // Each trial starts from a cold L2 (a write larger than the L2 first), as a
+    // batch of freshly mirrored payloads would, and times the stage alone; the
+    // reconstruction trials rerun on the entropy output left by the entropy
+    // trials.
+    DevBuf flush;
+    int l2 = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    const size_t fbytes = std::max<size_t>((size_t)l2 * 2, 64u << 20);
+    const bool do_flush = flush.ensure(fbytes);
     auto time_cfg = [&](const LaunchCfg &c, int stage) {
         decode_enqueue_stage(B, c, stage, s);   // warm
-        cudaEventRecord(e0, s);
-        for (int r = 0; r < 3; ++r) decode_enqueue_stage(B, c, stage, s);
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        return ms;
+        float total = 0.0f;
+        for (int r = 0; r < 3; ++r) {
+            if (do_flush) cudaMemsetAsync(flush.p, r, fbytes, s);
+            cudaEventRecord(e0, s);
+            decode_enqueue_stage(B, c, stage, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            total += ms;
+        }
+        return total;
     };
-    float best_ms = 1e30f;
+    // two interleaved rounds over the candidates, best time of each counts
     const int ent_opts[] = {4, 5, 6};
     const int rec_opts[] = {3, 4, 5};
-    for (int e : ent_opts) {
+    float ent_ms[3] = {1e30f, 1e30f, 1e30f}, rec_ms[3] = {1e30f, 1e30f, 1e30f};
+    for (int round = 0; round < 2; ++round)
+        for (int i = 0; i < 3; ++i) {
+            LaunchCfg c = best;
+            c.ent_ctas_per_sm = ent_opts[i];
+            ent_ms[i] = std::min(ent_ms[i], time_cfg(c, 0));
+        }
+    int be = 0;
+    for (int i = 1; i < 3; ++i) if (ent_ms[i] < ent_ms[be]) be = i;
+    best.ent_ctas_per_sm = ent_opts[be];
+    for (int round = 0; round < 2; ++round)
+        for (int i = 0; i < 3; ++i) {
+            LaunchCfg c = best;
+            c.rec_ctas_per_sm = rec_opts[i];
+            rec_ms[i] = std::min(rec_ms[i], time_cfg(c, 1));
+        }
+    int br = 0;
+    for (int i = 1; i < 3; ++i) if (rec_ms[i] < rec_ms[br]) br = i;
+    best.rec_ctas_per_sm = rec_opts[br];
+    // the whole decode with and without the long blocks on a second stream
+    {
         LaunchCfg c = best;
-        c.ent_ctas_per_sm = e;
-        float ms = time_cfg(c, 0);
-        if (ms < best_ms) { best_ms = ms; best = c; }
-    }
-    best_ms = 1e30f;
-    LaunchCfg base = best;
-    for (int r : rec_opts) {
-        LaunchCfg c = base;
-        c.rec_ctas_per_sm = r;
-        float ms = time_cfg(c, 1);
-        if (ms < best_ms) { best_ms = ms; best = c; }
+        c.split = false;
+        const float off = time_cfg(c, -1);
+        c.split = true;
+        const float on = time_cfg(c, -1);
+        best.split = on < off;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -529,6 +557,13 @@ void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint6
     if (launches) *launches = p ? p->launches : 0;
     if (blocks) *blocks = p ? p->blocks : 0;
     if (payload_bytes) *payload_bytes = p ? p->payload : 0;
+}
+
+void mc_b200_plan_config(const mc_b200_plan *p, int out[3]) {
+    if (!out) return;
+    out[0] = p ? p->cfg.ent_ctas_per_sm : 0;
+    out[1] = p ? p->cfg.rec_ctas_per_sm : 0;
+    out[2] = p ? (int)p->cfg.split : 0;
 }
 
 void mc_b200_plan_free(mc_b200_plan *p) {

@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
         if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
         if (L.st == S_DONE) {
             if (L.item >= 0) lane_finish(L, P);
-            const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.status + 2, 1u);
+            const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.counter, 1u);
             first = -1;
             L.item = -1;
             if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[nx] : nx);
@@ -539,6 +539,22 @@ __device__ __forceinline__ uint32_t to_u8(float v, int dc) {
 __device__ __forceinline__ uint32_t pack4(float2 a, float2 b, int dc) {
     return to_u8(a.x, dc) | (to_u8(a.y, dc) << 8) | (to_u8(b.x, dc) << 16) | (to_u8(b.y, dc) << 24);
 }
+// The same for a block whose voxels are all known to satisfy |v| < 2^21:
+// round half to even by the magic add, + dc, and a saturating pack (four
+// ints to u8, s0 in the low byte).
+__device__ __forceinline__ int rint_dc(float v, int dc) {
+    return __float_as_int(fadd(v, 12582912.0f)) - 0x4B400000 + dc;
+}
+__device__ __forceinline__ uint32_t pack4_fast(float2 a, float2 b, int dc) {
+    uint32_t t, d;
+    asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, 0;" : "=r"(t) : "r"(rint_dc(b.y, dc)), "r"(rint_dc(b.x, dc)));
+    asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(rint_dc(a.y, dc)), "r"(rint_dc(a.x, dc)), "r"(t));
+    return d;
+}
+// Every output voxel is a sum of at most 4096 terms coef * c[kz][z]c[ky][y]c[kx][x]
+// with |c| <= sqrt(2/16), so |v| <= L1(coef) * 0.0442; below this L1 norm
+// (with a factor-2 margin for rounding) every voxel takes the fast rounding.
+constexpr float kFastL1 = 2097152.0f / 0.04419417f;
 
 // Shared-memory row strides (floats / bytes), padded so that the lanes of a
 // warp that write the four outputs (m, m+1, 15-m, 14-m) of a line hit four
@@ -575,7 +591,9 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         // extents of the coefficient box: largest cz, cy, cx of any entry
         // (src/mc_codec.c:371-372)
         __shared__ int s_ext[3];
+        __shared__ float s_l1;
         if (tid < 3) s_ext[tid] = 0;
+        if (tid == 3) s_l1 = 0.0f;
         __syncthreads();
         int mz = 0, my = 0, mx = 0;
         for (int j = tid; j < nnz; j += 128) {
@@ -584,15 +602,22 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             my = max(my, (int)((e >> 4) & 15));
             mx = max(mx, (int)(e & 15));
         }
-        atomicMax(&s_ext[0], mz);
-        atomicMax(&s_ext[1], my);
-        atomicMax(&s_ext[2], mx);
+        // one shared-memory atomic per warp
+        mz = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mz);
+        my = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)my);
+        mx = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mx);
+        if ((tid & 31) == 0) {
+            atomicMax(&s_ext[0], mz);
+            atomicMax(&s_ext[1], my);
+            atomicMax(&s_ext[2], mx);
+        }
         __syncthreads();
         const int E = s_ext[0] + 1, Y = s_ext[1] + 1, X = s_ext[2] + 1;
         const QTab &qt = P.qtab[it.qslot];
         for (int i = tid; i < E * Y * X; i += 128) sB[i] = 0.0f;
         __syncthreads();
         // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
+        float l1 = 0.0f;
         for (int j = tid; j < nnz; j += 128) {
             const uint32_t e = entry_at(P, base, cap, h.ovf, j);
             const int idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFF;
@@ -604,8 +629,13 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             const float a = (float)(lv < 0 ? -lv : lv);
             const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
             sB[(cz * Y + cy) * X + cx] = lv < 0 ? -r : r;
+            l1 = fadd(l1, r);
         }
+        // the L1 norm only bounds the voxels: any summation order will do
+        for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xFFFFFFFFu, l1, o);
+        if ((tid & 31) == 0) atomicAdd(&s_l1, l1);
         __syncthreads();
+        const bool fast = s_l1 < kFastL1;
         // pass 1: lines along x (cz,cy), box -> A[cz][cy][x]; the output pair
         // (m, m+1) of one line accumulates as one packed pair
         const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
@@ -654,10 +684,17 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + y * kRowF + xg * 4), kPlaneB / 4, E, W, mh);
             uint32_t *row = reinterpret_cast<uint32_t *>(stage + y * 16 + xg * 4);
             constexpr int Z = kStageZ / 4;
-            row[m * Z] = pack4(add2(a.e0a, a.o0a), add2(a.e0b, a.o0b), dc);
-            row[(m + 1) * Z] = pack4(add2(a.e1a, a.o1a), add2(a.e1b, a.o1b), dc);
-            row[(15 - m) * Z] = pack4(sub2(a.e0a, a.o0a), sub2(a.e0b, a.o0b), dc);
-            row[(14 - m) * Z] = pack4(sub2(a.e1a, a.o1a), sub2(a.e1b, a.o1b), dc);
+            if (fast) {
+                row[m * Z] = pack4_fast(add2(a.e0a, a.o0a), add2(a.e0b, a.o0b), dc);
+                row[(m + 1) * Z] = pack4_fast(add2(a.e1a, a.o1a), add2(a.e1b, a.o1b), dc);
+                row[(15 - m) * Z] = pack4_fast(sub2(a.e0a, a.o0a), sub2(a.e0b, a.o0b), dc);
+                row[(14 - m) * Z] = pack4_fast(sub2(a.e1a, a.o1a), sub2(a.e1b, a.o1b), dc);
+            } else {
+                row[m * Z] = pack4(add2(a.e0a, a.o0a), add2(a.e0b, a.o0b), dc);
+                row[(m + 1) * Z] = pack4(add2(a.e1a, a.o1a), add2(a.e1b, a.o1b), dc);
+                row[(15 - m) * Z] = pack4(sub2(a.e0a, a.o0a), sub2(a.e0b, a.o0b), dc);
+                row[(14 - m) * Z] = pack4(sub2(a.e1a, a.o1a), sub2(a.e1b, a.o1b), dc);
+            }
         }
     }
     __syncthreads();
@@ -719,10 +756,12 @@ __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
     const int tid = threadIdx.x;
     const int npairs = (P.n + 1) / 2;
     for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
-        const int i0 = 2 * pr, i1 = 2 * pr + 1;
+        const int j0 = 2 * pr, j1 = 2 * pr + 1;
+        const int i0 = P.idx ? (int)P.idx[j0] : j0;
         reconstruct_block(P, i0, sA, sB, sStage0, sW);
         const DecItem a = P.items[i0];
-        if (i1 < P.n) {
+        if (j1 < P.n) {
+            const int i1 = P.idx ? (int)P.idx[j1] : j1;
             reconstruct_block(P, i1, sA, sB, sStage1, sW);
             const DecItem b = P.items[i1];
             if (pairable(a, b)) {

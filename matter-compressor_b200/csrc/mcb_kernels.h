@@ -11,6 +11,7 @@ namespace mcb {
 struct LaunchCfg {
     int ent_ctas_per_sm = 5;   // entropy stage: CTAs of 4 warps per SM (<= 5: 44 KB smem)
     int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
+    bool split = false;        // long blocks on a second stream (batches large enough to split)
 };
 
 struct EntParams {
@@ -27,12 +28,13 @@ struct EntParams {
     uint32_t *pool_used;
     const QTab *qtab;
     const uint16_t *scan;      // scan position -> raster idx | band<<12
-    uint32_t *status;          // [0]: blocks whose stream was cut short, [1]: pool entries
-                               // used, [2]: work counter (all zero at launch)
+    uint32_t *status;          // [0]: blocks whose stream was cut short, [1]: pool entries used
+    uint32_t *counter;         // work counter of this launch, zero at launch
 };
 
 struct RecParams {
     const DecItem *items;
+    const uint32_t *idx;       // optional: the items to reconstruct (n of them), ascending; null = 0..n-1
     int n;
     const EntHdr *hdr;
     const uint64_t *base;

@@ -190,8 +190,10 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     ep.qtab = reinterpret_cast<const QTab *>(sc + kOffQtab);
     ep.scan = reinterpret_cast<const uint16_t *>(sc + kOffScan);
     ep.status = reinterpret_cast<uint32_t *>(sc + kOffStatus);
+    ep.counter = ep.status + 2;
     RecParams rp;
     rp.items = ep.items;
+    rp.idx = nullptr;
     rp.n = n;
     rp.hdr = ep.hdr;
     rp.base = ep.base;

@@ -157,10 +157,16 @@ static constexpr uint32_t kPoolEntries = 4u << 20;           // overflow pool, 1
 // sub-batch's entry count. The order within a sub-batch is longest payload
 // first (counting sort by length), so the lanes of a warp decode blocks of
 // similar size and the per-lane totals balance (longest-processing-time-first).
-static uint64_t batch_layout(DecodeBatch &B, const DecItem *h_items, int n, uint64_t *hb, uint32_t *order) {
+// Sub-batches with at least this many coded blocks split off their longest
+// sixteenth (see DecodeBatch::split).
+static constexpr int kSplitMin = 16384;
+
+static uint64_t batch_layout(DecodeBatch &B, const DecItem *h_items, int n, uint64_t *hb, uint32_t *order,
+                             uint32_t *recidx) {
     B.n = n;
     B.subs.clear();
     B.coded.clear();
+    B.split.clear();
     uint64_t max_acc = 1;
     int i0 = 0;
     while (i0 < n) {
@@ -191,21 +197,33 @@ static uint64_t batch_layout(DecodeBatch &B, const DecItem *h_items, int n, uint
             coded += h_items[i].len > 0;
         }
         B.coded.push_back(coded);   // absent blocks sort last: the first `coded` entries have payloads
+        const int k = coded >= kSplitMin ? coded / 16 : 0;
+        B.split.push_back(k);
+        // reconstruction lists: the split-off blocks ascending, then the rest ascending
+        const int m = r.second - r.first;
+        static thread_local std::vector<uint8_t> head;
+        head.assign((size_t)m, 0);
+        for (int j = 0; j < k; ++j) head[order[r.first + j]] = 1;
+        int a = 0, b = k;
+        for (int i = 0; i < m; ++i) recidx[r.first + (head[i] ? a++ : b++)] = (uint32_t)i;
     }
     return max_acc;
 }
 
 static bool batch_buffers(DecodeBatch &B, int n, uint64_t max_acc) {
-    return B.order.ensure(sizeof(uint32_t) * (size_t)n) && B.items.ensure(sizeof(DecItem) * (size_t)n) &&
+    return B.order.ensure(sizeof(uint32_t) * (size_t)n) && B.rec_idx.ensure(sizeof(uint32_t) * (size_t)n) &&
+           B.items.ensure(sizeof(DecItem) * (size_t)n) &&
            B.base.ensure(sizeof(uint64_t) * (size_t)n) && B.hdr.ensure(sizeof(EntHdr) * (size_t)n) &&
            B.arena.ensure(sizeof(uint32_t) * max_acc) && B.pool.ensure(sizeof(uint32_t) * kPoolEntries) &&
            B.status.ensure(16);
 }
 
-static bool batch_upload(DecodeBatch &B, const DecItem *items, const uint32_t *order, const uint64_t *hb, int n,
-                         cudaStream_t s) {
+static bool batch_upload(DecodeBatch &B, const DecItem *items, const uint32_t *order, const uint64_t *hb,
+                         const uint32_t *recidx, int n, cudaStream_t s) {
     return cuda_ok(cudaMemcpyAsync(B.items.p, items, sizeof(DecItem) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D items") &&
+           cuda_ok(cudaMemcpyAsync(B.rec_idx.p, recidx, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s),
+                   "H2D rec idx") &&
            cuda_ok(cudaMemcpyAsync(B.order.p, order, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s),
                    "H2D order") &&
            cuda_ok(cudaMemcpyAsync(B.base.p, hb, sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s),
@@ -217,10 +235,10 @@ bool decode_prepare(DecodeBatch &B, const DecItem *h_items, int n, cudaStream_t 
     B.subs.clear();
     if (n <= 0) return true;
     std::vector<uint64_t> hb((size_t)n);
-    std::vector<uint32_t> order((size_t)n);
-    const uint64_t max_acc = batch_layout(B, h_items, n, hb.data(), order.data());
+    std::vector<uint32_t> order((size_t)n), recidx((size_t)n);
+    const uint64_t max_acc = batch_layout(B, h_items, n, hb.data(), order.data(), recidx.data());
     // synchronous copies: the host arrays may be pageable and short-lived
-    return batch_buffers(B, n, max_acc) && batch_upload(B, h_items, order.data(), hb.data(), n, s) &&
+    return batch_buffers(B, n, max_acc) && batch_upload(B, h_items, order.data(), hb.data(), recidx.data(), n, s) &&
            cuda_ok(cudaStreamSynchronize(s), "sync");
 }
 
@@ -228,12 +246,14 @@ bool decode_prepare_staged(DecodeBatch &B, int n, cudaStream_t s) {
     B.n = n;
     B.subs.clear();
     if (n <= 0) return true;
-    if (!B.h_order.ensure(sizeof(uint32_t) * (size_t)n) || !B.h_base.ensure(sizeof(uint64_t) * (size_t)n))
+    if (!B.h_order.ensure(sizeof(uint32_t) * (size_t)n) || !B.h_base.ensure(sizeof(uint64_t) * (size_t)n) ||
+        !B.h_rec.ensure(sizeof(uint32_t) * (size_t)n))
         return false;
     const DecItem *items = B.h_items.as<DecItem>();
-    const uint64_t max_acc = batch_layout(B, items, n, B.h_base.as<uint64_t>(), B.h_order.as<uint32_t>());
+    const uint64_t max_acc =
+        batch_layout(B, items, n, B.h_base.as<uint64_t>(), B.h_order.as<uint32_t>(), B.h_rec.as<uint32_t>());
     return batch_buffers(B, n, max_acc) &&
-           batch_upload(B, items, B.h_order.as<uint32_t>(), B.h_base.as<uint64_t>(), n, s);
+           batch_upload(B, items, B.h_order.as<uint32_t>(), B.h_base.as<uint64_t>(), B.h_rec.as<uint32_t>(), n, s);
 }
 
 BlobSlot::~BlobSlot() {
@@ -251,13 +271,31 @@ bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s) {
     return decode_enqueue_stage(B, cfg, -1, s);
 }
 
+DecodeBatch::~DecodeBatch() {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+}
+
+static bool side_stream(DecodeBatch &B) {
+    if (B.side) return true;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    return cuda_ok(cudaStreamCreateWithPriority(&B.side, cudaStreamNonBlocking, greatest), "stream") &&
+           cuda_ok(cudaEventCreateWithFlags(&B.ev_fork, cudaEventDisableTiming), "event") &&
+           cuda_ok(cudaEventCreateWithFlags(&B.ev_join, cudaEventDisableTiming), "event");
+}
+
 bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaStream_t s) {
     Runtime *R = runtime();
     if (!R) return false;
     const bool ent = stage != 1, rec = stage != 0;
     if (ent && !cuda_ok(cudaMemsetAsync(B.status.p, 0, 16, s), "memset")) return false;
+    uint32_t *status = B.status.as<uint32_t>();
     for (size_t si = 0; si < B.subs.size(); ++si) {
         const int i0 = B.subs[si].first, m = B.subs[si].second - B.subs[si].first;
+        const int k = cfg.split ? B.split[si] : 0;
+        if (k && !side_stream(B)) return false;
         EntParams ep;
         ep.items = B.items.as<DecItem>() + i0;
         ep.order = B.order.as<uint32_t>() + i0;
@@ -268,15 +306,14 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         ep.hdr = B.hdr.as<EntHdr>() + i0;
         ep.pool = B.pool.as<uint32_t>();
         ep.pool_cap = kPoolEntries;
-        ep.pool_used = B.status.as<uint32_t>() + 1;
+        ep.pool_used = status + 1;
         ep.qtab = R->d_qtab;
         ep.scan = R->d_scan;
-        ep.status = B.status.as<uint32_t>();
-        // each sub-batch's entropy launch starts its work counter at zero
-        if (ent && si > 0 && !cuda_ok(cudaMemsetAsync(B.status.as<uint32_t>() + 2, 0, 4, s), "memset")) return false;
-        if (ent && !cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
+        ep.status = status;
+        ep.counter = status + 2;
         RecParams rp;
         rp.items = B.items.as<DecItem>() + i0;
+        rp.idx = nullptr;
         rp.n = m;
         rp.hdr = B.hdr.as<EntHdr>() + i0;
         rp.base = B.base.as<uint64_t>() + i0;
@@ -284,7 +321,34 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         rp.pool = B.pool.as<uint32_t>();
         rp.qtab = R->d_qtab;
         rp.scan = R->d_scan;
-        if (rec && !cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
+        // each sub-batch's entropy launches start their work counters at zero
+        if (ent && si > 0 && !cuda_ok(cudaMemsetAsync(status + 2, 0, 8, s), "memset")) return false;
+        if (!k) {
+            if (ent && !cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
+            if (rec && !cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;
+            continue;
+        }
+        // fork: the longest k blocks on the side stream, the rest here
+        if (!cuda_ok(cudaEventRecord(B.ev_fork, s), "event record") ||
+            !cuda_ok(cudaStreamWaitEvent(B.side, B.ev_fork, 0), "stream wait"))
+            return false;
+        EntParams ea = ep, eb = ep;
+        ea.ncoded = k;
+        ea.counter = status + 3;
+        eb.order = ep.order + k;
+        eb.ncoded = ep.ncoded - k;
+        RecParams ra = rp, rb = rp;
+        ra.idx = B.rec_idx.as<uint32_t>() + i0;
+        ra.n = k;
+        rb.idx = ra.idx + k;
+        rb.n = m - k;
+        if (ent && !cuda_ok(launch_entropy(ea, cfg, B.side), "entropy launch")) return false;
+        if (rec && !cuda_ok(launch_reconstruct(ra, cfg, B.side), "reconstruct launch")) return false;
+        if (ent && !cuda_ok(launch_entropy(eb, cfg, s), "entropy launch")) return false;
+        if (rec && !cuda_ok(launch_reconstruct(rb, cfg, s), "reconstruct launch")) return false;
+        if (!cuda_ok(cudaEventRecord(B.ev_join, B.side), "event record") ||
+            !cuda_ok(cudaStreamWaitEvent(s, B.ev_join, 0), "stream wait"))
+            return false;
     }
     return true;
 }

@@ -62,11 +62,23 @@ int qslot(float q);
 // host item array and uploads items and offsets; decode_enqueue launches the
 // two stages (capturable into a CUDA graph).
 struct DecodeBatch {
-    DevBuf items, order, base, hdr, arena, pool, status;
-    HostBuf h_items, h_order, h_base, h_status;   // pinned staging of decode_prepare_staged
+    DevBuf items, order, base, hdr, arena, pool, status, rec_idx;
+    HostBuf h_items, h_order, h_base, h_status, h_rec;   // pinned staging of decode_prepare_staged
     int n = 0;
     std::vector<std::pair<int, int>> subs;   // [i0, i1) ranges that fit the arena
     std::vector<int> coded;                  // per sub-batch: items with a payload
+    // Per sub-batch: the longest `split` coded blocks (the head of the
+    // processing order) decode and reconstruct on a second, high-priority
+    // stream, so that the long serial chains of their entropy decode overlap
+    // the reconstruction of everything else. rec_idx lists, per sub-batch,
+    // those blocks' items ascending, then the other items ascending.
+    std::vector<int> split;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    DecodeBatch() = default;
+    DecodeBatch(const DecodeBatch &) = delete;
+    DecodeBatch &operator=(const DecodeBatch &) = delete;
+    ~DecodeBatch();
 };
 // One stage of the host-blob decode pipeline: its own stream, batch and
 // device buffers, reused once the event of its previous group has fired.

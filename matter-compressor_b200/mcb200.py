@@ -110,6 +110,7 @@ class McLib:
                 "mc_b200_plan_launch_stage": (i, [vp, i, vp]),
                 "mc_b200_plan_info": (None, [vp, C.POINTER(i), C.POINTER(lg), C.POINTER(u64)]),
                 "mc_b200_plan_free": (None, [vp]),
+                "mc_b200_plan_config": (None, [vp, vp]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
                 "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
                 "mc_b200_server_open": (vp, [vp, sz, sz, i]),
@@ -340,6 +341,12 @@ class Plan:
         n, b, pb = C.c_int(), C.c_long(), C.c_uint64()
         self.lib.L.mc_b200_plan_info(self.p, C.byref(n), C.byref(b), C.byref(pb))
         return n.value, b.value, pb.value
+
+    def config(self):
+        out = np.zeros(3, np.int32)
+        self.lib.L.mc_b200_plan_config(self.p, _ptr(out))
+        return {"entropy_ctas_per_sm": int(out[0]), "reconstruct_ctas_per_sm": int(out[1]),
+                "long_blocks_on_second_stream": bool(out[2])}
 
     def free(self):
         if self.p:
