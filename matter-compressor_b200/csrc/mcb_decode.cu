@@ -502,17 +502,24 @@ __device__ __forceinline__ Acc4 lines4(const float4 *in, int ks, int K, const fl
     Acc4 a;
     const float2 z = make_float2(0.f, 0.f);
     a.e0a = a.e0b = a.e1a = a.e1b = a.o0a = a.o0b = a.o1a = a.o1b = z;
-    for (int k = 0; k < K; k += 2) {
+    // (even, odd) pairs of k without a per-step guard, then the last even k
+    int k = 0;
+#pragma unroll 2
+    for (; k + 1 < K; k += 2) {
         const float4 v = in[k * ks], w = W[k * 8 + mh];
         const float2 w0 = lo2(w), w1 = hi2(w);
         a.e0a = madd2(a.e0a, w0, lo2(v)); a.e0b = madd2(a.e0b, w0, hi2(v));
         a.e1a = madd2(a.e1a, w1, lo2(v)); a.e1b = madd2(a.e1b, w1, hi2(v));
-        if (k + 1 < K) {
-            const float4 u = in[(k + 1) * ks], x = W[(k + 1) * 8 + mh];
-            const float2 x0 = lo2(x), x1 = hi2(x);
-            a.o0a = madd2(a.o0a, x0, lo2(u)); a.o0b = madd2(a.o0b, x0, hi2(u));
-            a.o1a = madd2(a.o1a, x1, lo2(u)); a.o1b = madd2(a.o1b, x1, hi2(u));
-        }
+        const float4 u = in[(k + 1) * ks], x = W[(k + 1) * 8 + mh];
+        const float2 x0 = lo2(x), x1 = hi2(x);
+        a.o0a = madd2(a.o0a, x0, lo2(u)); a.o0b = madd2(a.o0b, x0, hi2(u));
+        a.o1a = madd2(a.o1a, x1, lo2(u)); a.o1b = madd2(a.o1b, x1, hi2(u));
+    }
+    if (k < K) {
+        const float4 v = in[k * ks], w = W[k * 8 + mh];
+        const float2 w0 = lo2(w), w1 = hi2(w);
+        a.e0a = madd2(a.e0a, w0, lo2(v)); a.e0b = madd2(a.e0b, w0, hi2(v));
+        a.e1a = madd2(a.e1a, w1, lo2(v)); a.e1b = madd2(a.e1b, w1, hi2(v));
     }
     return a;
 }
@@ -568,7 +575,7 @@ constexpr int kStageBytes = 16 * kStageZ;
 // output pair (m, m+1) = 2*(t&3) of every line it touches; its cosine weights
 // come from the shared table W.
 __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, float *sA, float *sB,
-                                                  uint8_t *stage, const float4 *W) {
+                                                  uint8_t *stage, const float4 *W, const float2 *W1) {
     const int tid = threadIdx.x;
     const int m = (tid & 3) * 2;
     const DecItem it = P.items[item];
@@ -643,15 +650,15 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             const int line = t >> 2;
             const float *in = sB + line * X;
             float2 e = make_float2(0.f, 0.f), o = e;
-            for (int k = 0; k < X; k += 2) {
+            int k = 0;
+            for (; k + 1 < X; k += 2) {
+                const float v = in[k], u = in[k + 1];
+                e = madd2(e, W1[k * 8 + mh], make_float2(v, v));
+                o = madd2(o, W1[(k + 1) * 8 + mh], make_float2(u, u));
+            }
+            if (k < X) {
                 const float v = in[k];
-                const float4 w = W[k * 8 + mh];
-                e = madd2(e, make_float2(w.x, w.z), make_float2(v, v));
-                if (k + 1 < X) {
-                    const float u = in[k + 1];
-                    const float4 x = W[(k + 1) * 8 + mh];
-                    o = madd2(o, make_float2(x.x, x.z), make_float2(u, u));
-                }
+                e = madd2(e, W1[k * 8 + mh], make_float2(v, v));
             }
             const float2 sum = add2(e, o), dif = sub2(e, o);
             float *out = sA + line * kRowF;
@@ -747,10 +754,12 @@ __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
     __shared__ __align__(16) float sB[16 * kPlaneB];
     __shared__ __align__(16) uint8_t sStage0[kStageBytes];
     __shared__ __align__(16) float4 sW[16 * 8];   // [k][m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}
+    __shared__ __align__(8) float2 sW1[16 * 8];   // [k][m/2] = {c[k][m], c[k][m+1]}
     uint8_t *const sStage1 = reinterpret_cast<uint8_t *>(sA);
     for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
+        sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
     __syncthreads();
     const int tid = threadIdx.x;
@@ -758,11 +767,11 @@ __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
     for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
         const int j0 = 2 * pr, j1 = 2 * pr + 1;
         const int i0 = P.idx ? (int)P.idx[j0] : j0;
-        reconstruct_block(P, i0, sA, sB, sStage0, sW);
+        reconstruct_block(P, i0, sA, sB, sStage0, sW, sW1);
         const DecItem a = P.items[i0];
         if (j1 < P.n) {
             const int i1 = P.idx ? (int)P.idx[j1] : j1;
-            reconstruct_block(P, i1, sA, sB, sStage1, sW);
+            reconstruct_block(P, i1, sA, sB, sStage1, sW, sW1);
             const DecItem b = P.items[i1];
             if (pairable(a, b)) {
                 uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
