@@ -474,6 +474,28 @@ def run_b200(args, d):
             torch.cuda.synchronize()
             stage_ms[stage] += e0.elapsed_time(e1) / args.steps
 
+    # the whole decode under each stage layout the autotuner chose among,
+    # its entropy and reconstruction shapes kept (the chosen layout is the step above)
+    layout_ms = {}
+    for stages in plan.STAGES:
+        if plan.set_config(plan_cfg["entropy_ctas_per_sm"], plan_cfg["reconstruct_ctas_per_sm"], stages) != 0:
+            continue
+        for k in range(2):
+            plan.launch(s.cuda_stream)
+        tot = 0.0
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            plan.launch(s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        layout_ms[stages] = round(tot / args.steps, 4)
+    plan.set_config(plan_cfg["entropy_ctas_per_sm"], plan_cfg["reconstruct_ctas_per_sm"], plan_cfg["stages"])
+    plan.launch(s.cuda_stream)
+    torch.cuda.synchronize()
+
     # bit-exactness spot check against the oracle on one chunk (rank 0)
     exact = None
     if d.rank == 0:
@@ -548,6 +570,7 @@ def run_b200(args, d):
         "latency": {"api": "mc_archive_decode_block (plain per-call drop-in, host buffer)",
                     "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[int(len(lat) * 0.99) - 1], 4)},
         "blocks_per_step": blocks, "payload_bytes_per_step": payload, "launch_config": plan_cfg,
+        "stage_layout_ms": layout_ms,
         "clocks": clk,
         "cpu_baseline": cpu,
     }

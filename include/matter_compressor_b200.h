@@ -153,8 +153,13 @@ int  mc_b200_plan_launch_stage(mc_b200_plan *p, int stage, void *stream);
 /* Kernel launches per replay, blocks decoded, and total payload bytes. */
 void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes);
 /* The launch shape the plan's autotuner chose: entropy CTAs per SM,
- * reconstruction CTAs per SM, and 1 if the longest blocks run on a second stream. */
+ * reconstruction CTAs per SM, and the stage layout: 0 two kernels in sequence,
+ * 1 the longest blocks on a second stream, 2 both stages in one persistent
+ * kernel. */
 void mc_b200_plan_config(const mc_b200_plan *p, int out[3]);
+/* Replace the autotuner's choice (same layout as mc_b200_plan_config) and
+ * recapture the plan. 0 on success, -1 on bad arguments or a CUDA error. */
+int  mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]);
 void mc_b200_plan_free(mc_b200_plan *p);
 
 /* Batched append: encode n chunks (chunk i's 256^3 voxels at HOST vox[i], or

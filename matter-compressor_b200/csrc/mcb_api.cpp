@@ -204,20 +204,56 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
     int br = 0;
     for (int i = 1; i < 3; ++i) if (rec_ms[i] < rec_ms[br]) br = i;
     best.rec_ctas_per_sm = rec_opts[br];
-    // the whole decode with and without the long blocks on a second stream
+    // the whole decode: separate kernels, the long blocks on a second
+    // stream, or both stages in one persistent kernel (two rounds, best of each)
     {
-        LaunchCfg c = best;
-        c.split = false;
-        const float off = time_cfg(c, -1);
-        c.split = true;
-        const float on = time_cfg(c, -1);
-        best.split = on < off;
+        float t[3] = {1e30f, 1e30f, 1e30f};
+        for (int round = 0; round < 2; ++round)
+            for (int mode = 0; mode < 3; ++mode) {
+                LaunchCfg c = best;
+                c.split = mode == 1;
+                c.fused = mode == 2;
+                if (c.fused && fused_grid(c) <= 0) continue;
+                t[mode] = std::min(t[mode], time_cfg(c, -1));
+            }
+        int bm = t[2] < t[0] && t[2] < t[1] ? 2 : (t[1] < t[0] ? 1 : 0);
+        // MC_B200_STAGES=sequential|split|fused overrides the choice
+        if (const char *f = getenv("MC_B200_STAGES")) {
+            if (!strcmp(f, "sequential")) bm = 0;
+            else if (!strcmp(f, "split")) bm = 1;
+            else if (!strcmp(f, "fused") && t[2] < 1e30f) bm = 2;
+        }
+        best.split = bm == 1;
+        best.fused = bm == 2;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tuned[key] = best;
     return best;
+}
+
+// (Re)capture the plan's launches with its current configuration.
+bool plan_capture(mc_b200_plan *p) {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->exec = nullptr;
+    p->graph = nullptr;
+    cudaStream_t cs = nullptr;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream") &&
+              cuda_ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture") &&
+              decode_enqueue(p->batch, p->cfg, cs);
+    cudaGraph_t g = nullptr;
+    if (cs) {
+        cudaError_t ce = cudaStreamEndCapture(cs, &g);
+        ok = ok && cuda_ok(ce, "end capture") && cuda_ok(cudaGraphInstantiate(&p->exec, g, 0), "instantiate");
+        cudaStreamDestroy(cs);
+    }
+    p->graph = g;
+    p->launches = 0;
+    for (size_t si = 0; si < p->batch.subs.size(); ++si)   // two kernels a sub-batch, four when split
+        p->launches += !p->cfg.fused && p->cfg.split && p->batch.split[si] ? 4 : 2;
+    return ok;
 }
 
 }  // namespace
@@ -521,17 +557,7 @@ mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *offs, in
     }
     if (!decode_prepare(p->batch, items.data(), (int)items.size(), L->stream)) { delete p; return nullptr; }
     p->cfg = autotune(p->batch, q_major, L->stream);
-    cudaStream_t cs = nullptr;
-    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream") &&
-              cuda_ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture") &&
-              decode_enqueue(p->batch, p->cfg, cs);
-    cudaGraph_t g = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(cs, &g);
-    ok = ok && cuda_ok(ce, "end capture") && cuda_ok(cudaGraphInstantiate(&p->exec, g, 0), "instantiate");
-    if (cs) cudaStreamDestroy(cs);
-    p->graph = g;
-    if (!ok) { mc_b200_plan_free(p); return nullptr; }
-    p->launches = 2 * (int)p->batch.subs.size();
+    if (!plan_capture(p)) { mc_b200_plan_free(p); return nullptr; }
     return p;
 }
 
@@ -563,7 +589,25 @@ void mc_b200_plan_config(const mc_b200_plan *p, int out[3]) {
     if (!out) return;
     out[0] = p ? p->cfg.ent_ctas_per_sm : 0;
     out[1] = p ? p->cfg.rec_ctas_per_sm : 0;
-    out[2] = p ? (int)p->cfg.split : 0;
+    out[2] = p ? (p->cfg.fused ? 2 : (int)p->cfg.split) : 0;
+}
+
+int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
+    if (!p || !cfg || cfg[0] < 1 || cfg[0] > 16 || cfg[1] < 1 || cfg[1] > 16 || cfg[2] < 0 || cfg[2] > 2) {
+        set_error("plan_set_config: bad arguments");
+        return -1;
+    }
+    LaunchCfg c = p->cfg;
+    c.ent_ctas_per_sm = cfg[0];
+    c.rec_ctas_per_sm = cfg[1];
+    c.split = cfg[2] == 1;
+    c.fused = cfg[2] == 2;
+    if (c.fused && fused_grid(c) <= 0) {
+        set_error("plan_set_config: the fused kernel cannot launch on this device");
+        return -1;
+    }
+    p->cfg = c;
+    return plan_capture(p) ? 0 : -1;
 }
 
 void mc_b200_plan_free(mc_b200_plan *p) {

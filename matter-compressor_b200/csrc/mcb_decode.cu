@@ -524,9 +524,22 @@ __device__ __forceinline__ Acc4 lines4(const float4 *in, int ks, int K, const fl
     return a;
 }
 
+// Entry j of a block. CG: read through L2 only (__ldcg), for entries that
+// another SM may have written during this kernel (the fused decode): a line
+// this SM cached earlier for a neighbouring block must not be reused.
+template <bool CG>
 __device__ __forceinline__ uint32_t entry_at(const RecParams &P, uint64_t base, uint32_t cap, uint32_t ovf, uint32_t j) {
-    if (j < cap) return P.arena[base + j];
-    return ovf == 0xFFFFFFFFu ? 0u : P.pool[ovf + (j - cap)];
+    if (j < cap) return CG ? __ldcg(P.arena + base + j) : P.arena[base + j];
+    if (ovf == 0xFFFFFFFFu) return 0u;
+    return CG ? __ldcg(P.pool + ovf + (j - cap)) : P.pool[ovf + (j - cap)];
+}
+template <bool CG>
+__device__ __forceinline__ EntHdr load_hdr(const EntHdr *h) {
+    if (!CG) return *h;
+    const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(h));
+    EntHdr r;
+    memcpy(&r, &v, sizeof r);
+    return r;
 }
 
 // (int)lrintf(v) + dc clamped to u8 (src/mc_codec.c:766-769). Adding 1.5*2^23
@@ -574,12 +587,13 @@ constexpr int kStageBytes = 16 * kStageZ;
 // Reconstruct one block into a stage (z slices of kStageZ bytes). Thread t owns the
 // output pair (m, m+1) = 2*(t&3) of every line it touches; its cosine weights
 // come from the shared table W.
+template <bool CG>
 __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, float *sA, float *sB,
                                                   uint8_t *stage, const float4 *W, const float2 *W1) {
     const int tid = threadIdx.x;
     const int m = (tid & 3) * 2;
     const DecItem it = P.items[item];
-    const EntHdr h = P.hdr[item];
+    const EntHdr h = load_hdr<CG>(P.hdr + item);
     const uint64_t base = P.base[item];
     const uint32_t cap = entry_cap(it.len);
     // the header comes from k_entropy; the guards keep every index below
@@ -604,7 +618,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         __syncthreads();
         int mz = 0, my = 0, mx = 0;
         for (int j = tid; j < nnz; j += 128) {
-            const uint32_t e = __ldg(P.scan + (entry_at(P, base, cap, h.ovf, j) & 0xFFFu)) & 0xFFFu;
+            const uint32_t e = __ldg(P.scan + (entry_at<CG>(P, base, cap, h.ovf, j) & 0xFFFu)) & 0xFFFu;
             mz = max(mz, (int)((e >> 8) & 15));
             my = max(my, (int)((e >> 4) & 15));
             mx = max(mx, (int)(e & 15));
@@ -626,7 +640,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
         float l1 = 0.0f;
         for (int j = tid; j < nnz; j += 128) {
-            const uint32_t e = entry_at(P, base, cap, h.ovf, j);
+            const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
             const int idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFF;
             const int lv = (int16_t)(e >> 16);
             if (!lv) continue;
@@ -709,8 +723,8 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         // corrections in stream order: a position may repeat, each
         // application clamps (src/mc_codec.c:775-781)
         for (int c = 0; c < ncorr; ++c) {
-            const uint32_t pos = entry_at(P, base, cap, h.ovf, nnz + 2 * c);
-            const uint32_t d = entry_at(P, base, cap, h.ovf, nnz + 2 * c + 1);
+            const uint32_t pos = entry_at<CG>(P, base, cap, h.ovf, nnz + 2 * c);
+            const uint32_t d = entry_at<CG>(P, base, cap, h.ovf, nnz + 2 * c + 1);
             if (pos >= (uint32_t)kN3) break;
             uint8_t &vox = stage[(pos >> 8) * kStageZ + (pos & 255)];
             const int v = (int)((uint32_t)vox + d);
@@ -767,11 +781,11 @@ __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
     for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
         const int j0 = 2 * pr, j1 = 2 * pr + 1;
         const int i0 = P.idx ? (int)P.idx[j0] : j0;
-        reconstruct_block(P, i0, sA, sB, sStage0, sW, sW1);
+        reconstruct_block<false>(P, i0, sA, sB, sStage0, sW, sW1);
         const DecItem a = P.items[i0];
         if (j1 < P.n) {
             const int i1 = P.idx ? (int)P.idx[j1] : j1;
-            reconstruct_block(P, i1, sA, sB, sStage1, sW, sW1);
+            reconstruct_block<false>(P, i1, sA, sB, sStage1, sW, sW1);
             const DecItem b = P.items[i1];
             if (pairable(a, b)) {
                 uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
@@ -788,6 +802,196 @@ __global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
         } else {
             store_block(a, sStage0);
         }
+        __syncthreads();
+    }
+}
+
+
+// ---------------------------------------------------------------- fused decode
+// One persistent kernel for both stages. Every CTA first runs entropy lanes
+// (the k_entropy loop) until the shared block queue is drained. Blocks are
+// reconstructed in the pairs k_reconstruct uses (items 2j, 2j+1, x-neighbours
+// inside a chunk): the block that completes a pair -- an absent block at
+// kernel start, a coded one when its lane finishes -- appends the pair to a
+// completion list. A CTA whose lanes are all idle reconstructs pairs in list
+// order, while CTAs that still hold long blocks finish their entropy decode:
+// the tail of the entropy stage overlaps the reconstruction of everything
+// else, and the entries of a finished block are read back while still in L2.
+// A CTA that claims a list position not yet written polls with a bounded
+// backoff; if the bound runs out it records the position and leaves, and
+// k_fused_tail (launched after, stream-ordered) reconstructs whatever was
+// recorded or never claimed. No wait is unbounded.
+struct FusedSmem {
+    union {
+        struct {
+            uint16_t bend[9];
+            uint32_t ctx[4][kCtxSlots][32];
+        } e;
+        struct {
+            float A[16 * 16 * kRowF];
+            float B[16 * kPlaneB];
+            uint8_t stage0[kStageBytes];
+        } r;
+    } u;
+    float4 W[16 * 8];
+    float2 W1[16 * 8];
+    int pair;
+};
+
+// Item `item` is ready for reconstruction; the last of its pair appends the pair.
+__device__ __forceinline__ void pair_ready(const FusedParams &F, int item) {
+    const uint32_t j = (uint32_t)item >> 1;
+    const uint32_t size = 2u * j + 1u < (uint32_t)F.r.n ? 2u : 1u;
+    __threadfence();   // this block's header and entries before the pair's count
+    if (atomicAdd(F.pair_cnt + j, 1u) + 1u == size) {
+        const uint32_t pos = atomicAdd(F.ws + kFusedDone, 1u);
+        __threadfence();   // the other block's results, seen through the count, before the list entry
+        atomicExch(F.rlist + pos, j + 1u);
+    }
+}
+
+// Pair at completion-list position p, or -1 if not written yet.
+__device__ __forceinline__ int list_pair(const FusedParams &F, uint32_t p) {
+    const uint32_t v = *reinterpret_cast<const volatile uint32_t *>(F.rlist + p);
+    return (int)v - 1;
+}
+
+template <bool CG>
+__device__ __forceinline__ void reconstruct_pair(const RecParams &P, int j, float *sA, float *sB, uint8_t *stage0,
+                                                 const float4 *W, const float2 *W1) {
+    const int tid = threadIdx.x;
+    uint8_t *const stage1 = reinterpret_cast<uint8_t *>(sA);   // sA is free once a block is staged
+    const int i0 = 2 * j, i1 = 2 * j + 1;
+    reconstruct_block<CG>(P, i0, sA, sB, stage0, W, W1);
+    const DecItem a = P.items[i0];
+    if (i1 < P.n) {
+        reconstruct_block<CG>(P, i1, sA, sB, stage1, W, W1);
+        const DecItem b = P.items[i1];
+        if (pairable(a, b)) {
+            uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
+            for (int r = tid; r < 256; r += 128) {
+                const int z = r >> 4, y = r & 15;
+                uint4 *row = reinterpret_cast<uint4 *>(dst + z * a.sz + y * a.sy);
+                row[0] = *reinterpret_cast<const uint4 *>(stage0 + z * kStageZ + y * 16);
+                row[1] = *reinterpret_cast<const uint4 *>(stage1 + z * kStageZ + y * 16);
+            }
+        } else {
+            store_block(a, stage0);
+            store_block(b, stage1);
+        }
+    } else {
+        store_block(a, stage0);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_decode_fused(FusedParams F) {
+    extern __shared__ __align__(16) uint8_t s_raw[];
+    FusedSmem &S = *reinterpret_cast<FusedSmem *>(s_raw);
+    const EntParams &P = F.e;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nlanes = gridDim.x * blockDim.x;
+    // absent blocks are ready at once
+    for (int q = P.ncoded + gtid; q < P.n; q += nlanes) pair_ready(F, (int)P.order[q]);
+    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
+        const uint32_t b = P.scan[i] >> 12;
+        if ((P.scan[i - 1] >> 12) != b) S.u.e.bend[b - 1] = (uint16_t)i;
+    }
+    for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
+        const int k = i >> 3, mm = (i & 7) * 2;
+        S.W[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
+        S.W1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
+    }
+    if (threadIdx.x == 0) { S.u.e.bend[7] = kN3; S.u.e.bend[8] = 0xFFFF; }
+    __syncthreads();
+
+    // ---- entropy: the k_entropy loop, each finished block marked ready
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t *ctx = &S.u.e.ctx[warp][0][lane];
+        const uint16_t *s_bend = S.u.e.bend;
+        LaneState L;
+        memset(&L, 0, sizeof L);
+        L.range = 0xFFFFFFFFu;
+        L.sel = kSel0;
+        L.st = S_DONE;
+        L.item = -1;
+        int first = gtid;
+        for (;;) {
+            const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
+            if (idle == 0xFFFFFFFFu) break;
+            while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
+                fast_step(L, P, ctx, s_bend);
+                fast_step(L, P, ctx, s_bend);
+            }
+            fast_step(L, P, ctx, s_bend);
+            if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
+            if (L.st == S_DONE) {
+                if (L.item >= 0) {
+                    lane_finish(L, P);
+                    pair_ready(F, L.item);
+                }
+                const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.counter, 1u);
+                first = -1;
+                L.item = -1;
+                if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, (int)P.order[nx]);
+                else L.st = S_IDLE;
+            }
+        }
+    }
+    __syncthreads();   // the shared memory changes hands
+
+    // ---- reconstruction over the completion list, one pair per claim
+    const uint32_t npairs = ((uint32_t)F.r.n + 1u) >> 1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int j = -1;
+            const uint32_t p = atomicAdd(F.ws + kFusedClaim, 1u);
+            if (p < npairs) {
+                j = list_pair(F, p);
+                uint32_t ns = 32;
+                for (uint32_t tries = 0; j < 0 && tries < F.spin_limit; ++tries) {
+                    __nanosleep(ns);
+                    if (ns < 1024) ns <<= 1;
+                    j = list_pair(F, p);
+                }
+                if (j < 0) F.ws[kFusedSkip0 + atomicAdd(F.ws + kFusedNSkip, 1u)] = p;   // k_fused_tail takes it
+                __threadfence();   // the pair's results after its list entry
+            }
+            S.pair = j;
+        }
+        __syncthreads();
+        const int j = S.pair;
+        if (j < 0) break;
+        reconstruct_pair<true>(F.r, j, S.u.r.A, S.u.r.B, S.u.r.stage0, S.W, S.W1);
+        __syncthreads();
+    }
+}
+
+// List positions that k_decode_fused recorded as given up or never claimed
+// (normally none): one pair per CTA step. Runs after it, stream-ordered, so
+// every pair is in the list.
+__global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
+    __shared__ __align__(16) float sA[16 * 16 * kRowF];
+    __shared__ __align__(16) float sB[16 * kPlaneB];
+    __shared__ __align__(16) uint8_t sStage0[kStageBytes];
+    __shared__ __align__(16) float4 sW[16 * 8];
+    __shared__ __align__(8) float2 sW1[16 * 8];
+    const uint32_t npairs = ((uint32_t)F.r.n + 1u) >> 1;
+    const uint32_t claimed = min(F.ws[kFusedClaim], npairs);
+    const uint32_t nsk = min(F.ws[kFusedNSkip], (uint32_t)kFusedMaxSkip);
+    const uint32_t work = nsk + (npairs - claimed);
+    if (blockIdx.x >= work) return;
+    for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
+        const int k = i >> 3, mm = (i & 7) * 2;
+        sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
+        sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
+    }
+    __syncthreads();
+    for (uint32_t w = blockIdx.x; w < work; w += gridDim.x) {
+        const uint32_t p = w < nsk ? F.ws[kFusedSkip0 + w] : claimed + (w - nsk);
+        const int j = p < npairs ? list_pair(F, p) : -1;
+        if (j < 0 || (uint32_t)j >= npairs) continue;   // every pair is listed by now
+        reconstruct_pair<false>(F.r, j, sA, sB, sStage0, sW, sW1);
         __syncthreads();
     }
 }
@@ -815,6 +1019,35 @@ cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_
     int cap = num_sms() * (cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5);
     if (blocks > cap) blocks = cap;
     k_entropy<W><<<blocks, W * 32, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+int fused_grid(const LaunchCfg &cfg) {
+    static int occ_by_dev[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &occ = occ_by_dev[dev & 63];
+    if (occ == 0) {
+        // dynamic shared memory above 48 KiB: opt in once per device
+        if (cudaFuncSetAttribute(k_decode_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(FusedSmem)) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_decode_fused, 128, sizeof(FusedSmem)) !=
+                cudaSuccess || occ < 1)
+            occ = -1;
+    }
+    if (occ < 0) return 0;
+    // every CTA resident at once: a CTA's waits are then on CTAs that run
+    const int per_sm = std::min(cfg.fused_ctas_per_sm > 0 ? cfg.fused_ctas_per_sm : 4, occ);
+    return std::min(num_sms() * per_sm, kFusedMaxSkip);
+}
+
+cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_t s) {
+    const int blocks = fused_grid(cfg);
+    if (blocks <= 0) return cudaErrorInvalidConfiguration;
+    k_decode_fused<<<blocks, 128, sizeof(FusedSmem), s>>>(f);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_fused_tail<<<num_sms(), 128, 0, s>>>(f);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,8 @@ struct LaunchCfg {
     int ent_ctas_per_sm = 5;   // entropy stage: CTAs of 4 warps per SM (<= 5: 44 KB smem)
     int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
     bool split = false;        // long blocks on a second stream (batches large enough to split)
+    bool fused = false;        // both stages in one persistent kernel (k_decode_fused)
+    int fused_ctas_per_sm = 4;
 };
 
 struct EntParams {
@@ -44,6 +46,26 @@ struct RecParams {
     const uint16_t *scan;      // scan position -> raster idx | band<<12
 };
 
+// Both stages in one persistent kernel: entropy lanes mark finished blocks
+// ready, the block completing a pair (2j, 2j+1) appends it to a completion
+// list, and CTAs whose lanes are idle reconstruct pairs from that list
+// (k_decode_fused); then a tail kernel for positions a CTA gave up waiting on.
+// Work area F.ws, zeroed before each launch: kFusedDone, kFusedClaim and
+// kFusedNSkip counters, kFusedMaxSkip skipped positions, then pair_cnt and
+// rlist (fused_ws_words(n) words in all).
+constexpr int kFusedDone = 0, kFusedClaim = 1, kFusedNSkip = 2, kFusedSkip0 = 4;
+constexpr int kFusedMaxSkip = 4096;   // also the largest grid
+inline size_t fused_ws_words(int n) { return (size_t)kFusedSkip0 + kFusedMaxSkip + 2 * (((size_t)n + 1) / 2); }
+struct FusedParams {
+    EntParams e;               // e.order holds the coded blocks first, then the absent ones
+    RecParams r;               // r.n: items of the batch; r.idx unused
+    uint32_t *ws;              // the work area
+    uint32_t *pair_cnt;        // ws + kFusedSkip0 + kFusedMaxSkip: blocks of pair j ready
+    uint32_t *rlist;           // pair_cnt + npairs: list position -> pair + 1, 0 until written
+    uint32_t spin_limit;       // polls of an unwritten position before giving up
+};
+int fused_grid(const LaunchCfg &cfg);   // CTAs of k_decode_fused (0: cannot launch)
+cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
 // ---- serving ----
 // One chunk's share of a request: a box of blocks, the request's voxel clip in

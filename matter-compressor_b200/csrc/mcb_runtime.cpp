@@ -215,7 +215,7 @@ static bool batch_buffers(DecodeBatch &B, int n, uint64_t max_acc) {
            B.items.ensure(sizeof(DecItem) * (size_t)n) &&
            B.base.ensure(sizeof(uint64_t) * (size_t)n) && B.hdr.ensure(sizeof(EntHdr) * (size_t)n) &&
            B.arena.ensure(sizeof(uint32_t) * max_acc) && B.pool.ensure(sizeof(uint32_t) * kPoolEntries) &&
-           B.status.ensure(16);
+           B.status.ensure(16) && B.fws.ensure(sizeof(uint32_t) * fused_ws_words(n));
 }
 
 static bool batch_upload(DecodeBatch &B, const DecItem *items, const uint32_t *order, const uint64_t *hb,
@@ -323,6 +323,20 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         rp.scan = R->d_scan;
         // each sub-batch's entropy launches start their work counters at zero
         if (ent && si > 0 && !cuda_ok(cudaMemsetAsync(status + 2, 0, 8, s), "memset")) return false;
+        if (cfg.fused && ent && rec) {
+            // both stages in one persistent kernel
+            FusedParams fp;
+            fp.e = ep;
+            fp.r = rp;
+            fp.ws = B.fws.as<uint32_t>();
+            fp.pair_cnt = fp.ws + kFusedSkip0 + kFusedMaxSkip;
+            fp.rlist = fp.pair_cnt + (m + 1) / 2;
+            fp.spin_limit = 1u << 15;   // polls of at most 1 us each
+            if (!cuda_ok(cudaMemsetAsync(fp.ws, 0, sizeof(uint32_t) * fused_ws_words(m), s), "memset") ||
+                !cuda_ok(launch_fused(fp, cfg, s), "fused decode launch"))
+                return false;
+            continue;
+        }
         if (!k) {
             if (ent && !cuda_ok(launch_entropy(ep, cfg, s), "entropy launch")) return false;
             if (rec && !cuda_ok(launch_reconstruct(rp, cfg, s), "reconstruct launch")) return false;

@@ -63,6 +63,7 @@ int qslot(float q);
 // two stages (capturable into a CUDA graph).
 struct DecodeBatch {
     DevBuf items, order, base, hdr, arena, pool, status, rec_idx;
+    DevBuf fws;   // work area of the fused decode kernel
     HostBuf h_items, h_order, h_base, h_status, h_rec;   // pinned staging of decode_prepare_staged
     int n = 0;
     std::vector<std::pair<int, int>> subs;   // [i0, i1) ranges that fit the arena

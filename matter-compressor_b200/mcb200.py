@@ -111,6 +111,7 @@ class McLib:
                 "mc_b200_plan_info": (None, [vp, C.POINTER(i), C.POINTER(lg), C.POINTER(u64)]),
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_plan_config": (None, [vp, vp]),
+                "mc_b200_plan_set_config": (i, [vp, vp]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
                 "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
                 "mc_b200_server_open": (vp, [vp, sz, sz, i]),
@@ -346,7 +347,16 @@ class Plan:
         out = np.zeros(3, np.int32)
         self.lib.L.mc_b200_plan_config(self.p, _ptr(out))
         return {"entropy_ctas_per_sm": int(out[0]), "reconstruct_ctas_per_sm": int(out[1]),
-                "long_blocks_on_second_stream": bool(out[2])}
+                "stages": ("sequential", "long_blocks_on_second_stream", "fused")[int(out[2])]}
+
+    STAGES = ("sequential", "long_blocks_on_second_stream", "fused")
+
+    def set_config(self, entropy_ctas_per_sm, reconstruct_ctas_per_sm, stages):
+        """Override the autotuned launch shape and recapture the plan."""
+        cfg = np.array([entropy_ctas_per_sm, reconstruct_ctas_per_sm, self.STAGES.index(stages)], np.int32)
+        rc = self.lib.L.mc_b200_plan_set_config(self.p, _ptr(cfg))
+        self.lib.check()
+        return rc
 
     def free(self):
         if self.p:

@@ -175,6 +175,40 @@ def test_synthetic_chunk_q6(gpu, oracle, tmp_path):
         plan.free()
 
 
+def test_plan_stage_layouts(gpu, oracle, tmp_path):
+    """Every stage layout of a decode plan -- two kernels in sequence, the long
+    blocks on a second stream, one fused persistent kernel -- gives the
+    oracle's voxels, on a batch with absent and all-air chunks, an odd number
+    of blocks per sub-batch pair boundary and chunks of two qualities."""
+    import torch
+    import volumes
+    with gpu.open(str(tmp_path / "f.mca"), 1024, 512, 256, 6.0) as a:
+        coords = [(0, 0, 0), (0, 0, 1), (0, 1, 2), (0, 1, 3)]
+        vox = [volumes.region(21 + i, (0, 256 * (c[1]), 256 * c[2]), (256, 256, 256), 0.4, device="cuda")
+               for i, c in enumerate(coords)]
+        vox[2].zero_()   # an all-air chunk
+        for c, v, q in zip(coords, vox, (6.0, 6.0, 6.0, 3.0)):
+            assert a.append_par(0, *c, v.cpu().numpy(), q) == 0
+        offs = [a.chunk_offset(0, *c) for c in coords] + [a.chunk_offset(0, 0, 0, 3)]   # the last one absent
+        data = np.fromfile(str(tmp_path / "f.mca"), np.uint8).tobytes()
+        want = np.concatenate([oracle.decode_chunk(data[o:o + shapes.blob_len(data, o)]) if o > 1
+                               else np.zeros(CHUNK, np.uint8) for o in offs])
+        d_out = torch.empty(len(offs) * CHUNK, dtype=torch.uint8, device="cuda")
+        plan = a.plan_chunks(offs, d_out.data_ptr())
+        try:
+            for stages in plan.STAGES:
+                for ent, rec in ((5, 4), (3, 2)):
+                    assert plan.set_config(ent, rec, stages) == 0
+                    assert plan.config()["stages"] == stages
+                    d_out.fill_(0xEE)
+                    for _ in range(2):   # the work area is reset by every replay
+                        plan.launch()
+                    torch.cuda.synchronize()
+                    assert np.array_equal(d_out.cpu().numpy(), want), (stages, ent, rec)
+        finally:
+            plan.free()
+
+
 def test_mixed_quality_batch(gpu, oracle, tmp_path):
     """Chunks of different q in one batched append and one batched decode."""
     import torch
