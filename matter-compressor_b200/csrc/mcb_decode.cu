@@ -328,6 +328,11 @@ __device__ __forceinline__ void stg_if(bool pred, uint32_t *p, uint32_t v) {
 // refill, a second renormalisation byte, band change, end of scan, end of an
 // Exp-Golomb prefix, entry-list overflow) share one branch. A lane in any
 // other state passes through unchanged.
+// INNER: every lane of the warp is live or idle (the first step of an inner
+// loop round). An idle lane's decoder fields are then don't-care -- it never
+// decodes again -- so only its state, its stores and the rare-event branch
+// stay guarded. A lane in a slow state needs every field kept.
+template <bool INNER>
 __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_bend) {
     const uint32_t st = L.st;
     const bool live = st <= F_EGP;
@@ -345,10 +350,10 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     // this bin
     const uint32_t p0 = L.pc;
     const uint32_t r0 = is_byp ? L.range >> 1 : (L.range >> 12) * p0;
-    const bool bit = live & (L.code >= r0);
+    const bool bit = (INNER || live) & (L.code >= r0);
     const uint32_t b = bit ? 1u : 0u;
     const uint32_t code = bit ? L.code - r0 : L.code;
-    const uint32_t range = !live ? L.range : ((bit & !is_byp) ? L.range - r0 : r0);
+    const uint32_t range = !(INNER || live) ? L.range : ((bit & !is_byp) ? L.range - r0 : r0);
     const uint32_t np0 = p0 + (uint32_t)((int)((bit ? 15u : 4096u) - p0) >> 4);
     sts_if(live & !is_byp, ctx + L.cc * 32, np0);
     // renormalisation, first byte (src/mc_codec.c:202)
@@ -359,8 +364,8 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     // next bin's context
     const uint32_t ncc = bit ? c1 : c0;
     const uint32_t nq = bit ? q1 : q0;
-    L.pc = live ? ((ncc == L.cc && !is_byp) ? np0 : nq) : L.pc;
-    L.cc = live ? ncc : L.cc;
+    L.pc = (INNER || live) ? ((ncc == L.cc && !is_byp) ? np0 : nq) : L.pc;
+    L.cc = (INNER || live) ? ncc : L.cc;
 
     // significance history (the flag leaving the 16-position window drops out of cnt)
     L.hist = is_sig ? (L.hist << 1) | b : L.hist;
@@ -368,7 +373,7 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     const uint32_t m = L.m;
     L.m = is_mag ? k1 : m;
     const bool esc = is_mag & bit & (L.k == 11);            // 12th rung set: Exp-Golomb tail
-    L.k = live ? (((is_mag | is_egp) & bit) ? k1 : 0u) : L.k;
+    L.k = (INNER || live) ? (((is_mag | is_egp) & bit) ? k1 : 0u) : L.k;
     L.ret = esc ? (uint32_t)R_MAG : L.ret;
     const uint32_t nst = is_sig ? b : (is_mag ? (bit ? (esc ? (uint32_t)F_EGP : (uint32_t)F_MAG) : (uint32_t)F_SIGN)
                                             : (is_sign ? (uint32_t)F_SIG : (uint32_t)F_EGP));
@@ -384,7 +389,7 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     const uint32_t np = L.p + (adv ? 1u : 0u);
     L.p = np;
     const bool event = adv & (np >= L.stop);
-    if ((L.sel == kSel0 + 4) | (L.range < (1u << 24)) | ovf | egend | event) {
+    if (live & ((L.sel == kSel0 + 4) | (L.range < (1u << 24)) | ovf | egend | event)) {
         if (L.sel == kSel0 + 4) refill(L);
         renorm(L);
         if (ovf && !put_entry(L, P, v)) return;   // corrupt stream: pool exhausted, block ends
@@ -435,10 +440,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
         const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
         if (idle == 0xFFFFFFFFu) break;
         while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
-            fast_step(L, P, ctx, s_bend);
-            fast_step(L, P, ctx, s_bend);
+            fast_step<true>(L, P, ctx, s_bend);    // every lane live or idle here
+            fast_step<false>(L, P, ctx, s_bend);   // the first step may have left a lane in a slow state
         }
-        fast_step(L, P, ctx, s_bend);
+        fast_step<false>(L, P, ctx, s_bend);
         if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
         if (L.st == S_DONE) {
             if (L.item >= 0) lane_finish(L, P);
@@ -576,11 +581,16 @@ __device__ __forceinline__ uint32_t pack4_fast(float2 a, float2 b, int dc) {
 // (with a factor-2 margin for rounding) every voxel takes the fast rounding.
 constexpr float kFastL1 = 2097152.0f / 0.04419417f;
 
-// Shared-memory row strides (floats / bytes), padded so that the lanes of a
-// warp that write the four outputs (m, m+1, 15-m, 14-m) of a line hit four
-// different banks.
-constexpr int kRowF = 20;            // A and B rows of 16 floats
-constexpr int kPlaneB = 16 * kRowF;  // one cz plane of B
+// Shared-memory layouts. A (pass-1 output) rows of 16 floats are padded to
+// kRowF so that the lanes of a warp that write the four outputs
+// (m, m+1, 15-m, 14-m) of a line hit different banks. B (pass-2 output) rows
+// are not padded: float4 group g of row y (in every cz plane) sits at group
+// g ^ bswz(y), so pass-3 loads (rows y, y+1 of one plane) are conflict-free
+// and pass-2 stores at most 2-way, in 4 KB less shared memory per CTA.
+constexpr int kRowF = 20;            // A rows of 16 floats
+constexpr int kRowB = 16;            // B rows
+constexpr int kPlaneB = 16 * kRowB;  // one cz plane of B
+__device__ __forceinline__ int bswz(int y) { return (y >> 1) & 3; }
 constexpr int kStageZ = 272;         // stage: one z slice of 16 rows of 16 bytes
 constexpr int kStageBytes = 16 * kStageZ;
 
@@ -687,22 +697,24 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             const int xg = (t >> 2) & 3, cz = t >> 4;
             const Acc4 a = lines4(reinterpret_cast<const float4 *>(sA + cz * Y * kRowF + xg * 4), kRowF / 4, Y,
                                   W, mh);
-            float4 *o = reinterpret_cast<float4 *>(sB + cz * kPlaneB + xg * 4);
-            constexpr int R = kRowF / 4;
+            // rows m, m+1 swizzle by bswz(m) = mh, rows 15-m, 14-m by 3 - mh
+            float *ob = sB + cz * kPlaneB;
+            const int ga = (xg ^ mh) << 2, gb = (xg ^ (3 - mh)) << 2;
             const float2 p0 = add2(a.e0a, a.o0a), p1 = add2(a.e0b, a.o0b);
             const float2 q0 = add2(a.e1a, a.o1a), q1 = add2(a.e1b, a.o1b);
             const float2 r0 = sub2(a.e0a, a.o0a), r1 = sub2(a.e0b, a.o0b);
             const float2 s0 = sub2(a.e1a, a.o1a), s1 = sub2(a.e1b, a.o1b);
-            o[m * R] = make_float4(p0.x, p0.y, p1.x, p1.y);
-            o[(m + 1) * R] = make_float4(q0.x, q0.y, q1.x, q1.y);
-            o[(15 - m) * R] = make_float4(r0.x, r0.y, r1.x, r1.y);
-            o[(14 - m) * R] = make_float4(s0.x, s0.y, s1.x, s1.y);
+            *reinterpret_cast<float4 *>(ob + m * kRowB + ga) = make_float4(p0.x, p0.y, p1.x, p1.y);
+            *reinterpret_cast<float4 *>(ob + (m + 1) * kRowB + ga) = make_float4(q0.x, q0.y, q1.x, q1.y);
+            *reinterpret_cast<float4 *>(ob + (15 - m) * kRowB + gb) = make_float4(r0.x, r0.y, r1.x, r1.y);
+            *reinterpret_cast<float4 *>(ob + (14 - m) * kRowB + gb) = make_float4(s0.x, s0.y, s1.x, s1.y);
         }
         __syncthreads();
         // pass 3: lines along z for 4 adjacent x, B[k][y][x..x+3] -> voxels
         for (int t = tid; t < 256; t += 128) {
             const int xg = (t >> 2) & 3, y = t >> 4;
-            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + y * kRowF + xg * 4), kPlaneB / 4, E, W, mh);
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + y * kRowB + ((xg ^ bswz(y)) << 2)), kPlaneB / 4,
+                                  E, W, mh);
             uint32_t *row = reinterpret_cast<uint32_t *>(stage + y * 16 + xg * 4);
             constexpr int Z = kStageZ / 4;
             if (fast) {
@@ -761,7 +773,7 @@ __device__ __forceinline__ bool pairable(const DecItem &a, const DecItem &b) {
            (a.sy & 31) == 0 && (a.sz & 31) == 0;
 }
 
-__global__ void __launch_bounds__(128) k_reconstruct(RecParams P) {
+__global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
     // sA: pass-1 output, then the second block's stage; sB: coefficient box,
     // then pass-2 output; sStage0: the first block's stage
     __shared__ __align__(16) float sA[16 * 16 * kRowF];
@@ -920,10 +932,10 @@ __global__ void __launch_bounds__(128) k_decode_fused(FusedParams F) {
             const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
             if (idle == 0xFFFFFFFFu) break;
             while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
-                fast_step(L, P, ctx, s_bend);
-                fast_step(L, P, ctx, s_bend);
+                fast_step<true>(L, P, ctx, s_bend);    // every lane live or idle here
+                fast_step<false>(L, P, ctx, s_bend);   // the first step may have left a lane in a slow state
             }
-            fast_step(L, P, ctx, s_bend);
+            fast_step<false>(L, P, ctx, s_bend);
             if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
             if (L.st == S_DONE) {
                 if (L.item >= 0) {
@@ -1056,6 +1068,14 @@ cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStr
     int blocks = (p.n + 1) / 2;   // one CTA step per pair of blocks
     int cap = num_sms() * (cfg.rec_ctas_per_sm > 0 ? cfg.rec_ctas_per_sm : 5);
     if (blocks > cap) blocks = cap;
+    static unsigned long long carve_set = 0;   // per device: the largest shared-memory carveout, 5 CTAs/SM fit
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(carve_set >> (dev & 63) & 1ull)) {
+        cudaFuncSetAttribute(k_reconstruct, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        carve_set |= 1ull << (dev & 63);
+    }
     k_reconstruct<<<blocks, 128, 0, s>>>(p);
     return cudaGetLastError();
 }
