@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--chunks", type=int, default=64)
     p.add_argument("--q", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="decode", choices=["decode", "serve", "regions", "encode"],
+    p.add_argument("--workload", default="decode", choices=["decode", "serve", "regions", "encode", "deblock"],
                    help="decode: batched chunk decode (the headline line); serve: request-serving sweep; "
                         "regions: dataloader region batch; encode: preset-ladder batched encode")
     p.add_argument("--rates", default="1000,10000,30000,100000,300000,1000000",
@@ -361,6 +361,121 @@ def run_regions(args):
             "cpu_baseline": cpu}
 
 
+def run_deblock(args):
+    """Decode-side deblocking of config 2's decoded chunks in HBM: the 64
+    decoded 256^3 chunks, each deblocked as its own volume, in one
+    mc_b200_deblock_dev call; the decoded bytes are restored before every
+    step (a 1 GiB device copy, which also evicts the L2)."""
+    from mcb200 import McLib
+    lib = McLib.product()
+    dev = torch.device("cuda", 0)
+    vox = make_volumes(chunk_seeds(0, args.chunks), dev)
+    td = tempfile.mkdtemp()
+    path = os.path.join(td, "deblock.mca")
+    a = lib.open(path, 256 * args.chunks, 256, 256, args.q)
+    assert a.append_chunks(0, [(0, 0, c) for c in range(args.chunks)], [vox[c].data_ptr() for c in range(args.chunks)],
+                           args.q, on_device=True) == 0
+    del vox
+    offs = [a.chunk_offset(0, 0, 0, c) for c in range(args.chunks)]
+    dec = torch.empty(args.chunks * CHUNK, dtype=torch.uint8, device=dev)
+    out = torch.empty_like(dec)
+    plan = a.plan_chunks(offs, dec.data_ptr())
+    s = torch.cuda.current_stream()
+    plan.launch(s.cuda_stream)
+    torch.cuda.synchronize()
+    n = args.chunks
+
+    def step():
+        out.copy_(dec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        assert lib.deblock_dev(out.data_ptr(), n, CHUNK, 256, 256, 256, args.q, s.cuda_stream) == 0
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks()
+    clocks.start()
+    times = [step() for _ in range(args.steps)]
+    clk = clocks.stop()
+    ms = statistics.median(times)
+    # decode and deblock back to back (graph-captured decode, then the three deblock kernels)
+    both = []
+    for k in range(args.steps):
+        out.fill_(k & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        plan.launch(s.cuda_stream)
+        lib.deblock_dev(dec.data_ptr(), n, CHUNK, 256, 256, 256, args.q, s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        both.append(e0.elapsed_time(e1))
+    plan.launch(s.cuda_stream)
+    torch.cuda.synchronize()
+    # exactness: the first and last chunk against the oracle's deblock of the same decoded voxels
+    from oracle import Oracle
+    orc = Oracle()
+    exact = True
+    for c in (0, n - 1):
+        src = dec[c * CHUNK:(c + 1) * CHUNK].cpu().numpy().reshape(256, 256, 256)
+        exact &= bool(np.array_equal(out[c * CHUNK:(c + 1) * CHUNK].cpu().numpy().reshape(256, 256, 256),
+                                     orc.deblock(src.copy(), args.q)))
+    # e2e: the drop-in mc_deblock on host chunks (host -> device -> host inside the call)
+    host = torch.empty(CHUNK, dtype=torch.uint8).pin_memory().numpy()
+    e2e = []
+    for k in range(max(3, args.steps // 2)):
+        host[:] = dec[(k % n) * CHUNK:(k % n + 1) * CHUNK].cpu().numpy()
+        t0 = time.perf_counter()
+        lib.deblock(host.reshape(256, 256, 256), args.q)
+        e2e.append(time.perf_counter() - t0)
+    e2e_gbs = CHUNK / statistics.median(e2e[1:]) / 1e9
+    plan.free()
+    a.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import REF_FAST_LIB
+        try:
+            import ctypes as C
+            R = C.CDLL(REF_FAST_LIB)
+            R.mc_deblock.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+            k, t_cpu = 0, 0.0
+            while t_cpu < 8.0 and k < n:
+                buf = np.zeros(CHUNK + 256 * 256, np.uint8)
+                buf[:CHUNK] = dec[k * CHUNK:(k + 1) * CHUNK].cpu().numpy()
+                t0 = time.perf_counter()
+                R.mc_deblock(buf.ctypes.data, 256, 256, 256, args.q)
+                t_cpu += time.perf_counter() - t0
+                k += 1
+            cpu = {"value": round(k * CHUNK / t_cpu / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
+                   "sample": f"the reference's mc_deblock (single-threaded, default-flag build) on {k} of the "
+                             f"same decoded 256^3 chunks"}
+        except (FileNotFoundError, OSError) as e:
+            cpu = {"value": None, "sample": f"unavailable: {e}"}
+    os.remove(path)
+    os.rmdir(td)
+    peak, peak_kind = hbm_peak()
+    vol = n * CHUNK
+    achieved = 2 * vol / (ms / 1e3) / 1e9
+    return {"metric": "deblocked GB/s of decoded volume (mc_deblock on device)", "workload": "deblock",
+            "value": round(vol / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic", "vs_baseline": None,
+            "config": {"workload": f"deblock {n} decoded 256^3 chunks (config 2 volumes, q={args.q:g}) in HBM, one "
+                                   f"volume per chunk, quality {args.q:g}",
+                       "l2": "1 GiB device copy before every step"},
+            "gpu_launches": 3 * args.steps,
+            "bit_exact_vs_oracle": exact,
+            "decode_and_deblock_gbs": round(vol / (statistics.median(both) / 1e3) / 1e9, 3),
+            "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": CHUNK,
+                    "d2h_bytes_per_step": CHUNK, "api": "mc_deblock (host volume, one 256^3 chunk per call)"},
+            "roofline": {"bound": "hbm", "kernel": "k_deblock_x + k_deblock_y + k_deblock_z",
+                         "achieved": round(achieved, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": 2 * vol},
+            "clocks": clk, "cpu_baseline": cpu}
+
+
 def run_encode(args):
     """Preset ladder: 8 chunks (30 % air) encoded at each of the 8 presets
     (q and tau from the preset table) in one batched append per level."""
@@ -582,8 +697,9 @@ def main():
     try:
         if args.workload != "decode":
             if d.world > 1:
-                raise SystemExit("the serve / regions / encode workloads run on one GPU")
-            res = {"serve": run_serve, "regions": run_regions, "encode": run_encode}[args.workload](args)
+                raise SystemExit("the serve / regions / encode / deblock workloads run on one GPU")
+            res = {"serve": run_serve, "regions": run_regions, "encode": run_encode,
+                   "deblock": run_deblock}[args.workload](args)
         else:
             res = run_reference(args, d) if args.impl == "reference" else run_b200(args, d)
         if res is not None:

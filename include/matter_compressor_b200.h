@@ -105,6 +105,9 @@ uint64_t mc_chunk_compute_hash(const uint8_t *blob, uint64_t blob_len);         
 long mc_verify_archive(const uint8_t *arc, size_t len, int verbose);                   /* :370 */
 int mc_archive_set_priors(mc_archive *a, const uint16_t plo[8][32], const uint16_t phi[8][32]); /* :377 */
 uint64_t mc_xxh64(const void *data, size_t len, uint64_t seed);            /* src/mc_codec.h:17 */
+/* Decode-side deblocking, in place on a dense HOST volume (staged through the
+ * device). A read past the volume's end, undefined in the reference, reads 0. */
+void mc_deblock(mc_u8 *vol, int nz, int ny, int nx, float quality);      /* src/matter_compressor.h:106 */
 
 /* ====================================================== part 2: additions */
 
@@ -157,6 +160,13 @@ void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint6
  * 1 the longest blocks on a second stream, 2 both stages in one persistent
  * kernel. */
 void mc_b200_plan_config(const mc_b200_plan *p, int out[3]);
+/* Deblocking filter (mc_deblock's arithmetic) in place on `count` dense DEVICE
+ * volumes of nz x ny x nx voxels, vol_stride bytes apart. 0 on success, -1 on
+ * bad arguments (count <= 65535 and each per-axis face count of one volume
+ * below 2^32) or a CUDA error. */
+int mc_b200_deblock_dev(mc_u8 *d_vol, int count, size_t vol_stride, int nz, int ny, int nx, float quality,
+                        void *stream);
+
 /* Replace the autotuner's choice (same layout as mc_b200_plan_config) and
  * recapture the plan. 0 on success, -1 on bad arguments or a CUDA error. */
 int  mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]);

@@ -425,6 +425,43 @@ int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
     return 0;
 }
 
+// ============================================================ deblocking
+// Gate and clamp from the quality, with the reference's float expressions
+// (src/mc_codec.c:577-578), evaluated on the host.
+static void deblock_params(float quality, int *beta, int *tc) {
+    *beta = (int)(3.0f * quality + 6.0f);
+    *tc = (int)(0.5f * quality + 1.0f);
+}
+
+int mc_b200_deblock_dev(mc_u8 *d_vol, int count, size_t vol_stride, int nz, int ny, int nx, float quality,
+                        void *stream) {
+    if (!d_vol || count <= 0 || nz <= 0 || ny <= 0 || nx <= 0) {
+        set_error("deblock: bad arguments");
+        return -1;
+    }
+    Lane *L = lane();
+    if (!L) return -1;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+    int beta, tc;
+    deblock_params(quality, &beta, &tc);
+    if (!cuda_ok(launch_deblock(d_vol, count, vol_stride, nz, ny, nx, beta, tc, s), "deblock launch")) return -1;
+    if (!stream && !finish(*L, nullptr)) return -1;
+    return 0;
+}
+
+void mc_deblock(mc_u8 *vol, int nz, int ny, int nx, float quality) {
+    if (!vol || nz <= 0 || ny <= 0 || nx <= 0) return;
+    Lane *L = lane();
+    if (!L) return;   // no device: the volume stays as it was, the error says why
+    const size_t n = (size_t)nz * ny * nx;
+    if (!L->out.ensure(n)) return;
+    int beta, tc;
+    deblock_params(quality, &beta, &tc);
+    cuda_ok(cudaMemcpyAsync(L->out.p, vol, n, cudaMemcpyHostToDevice, L->stream), "H2D") &&
+        cuda_ok(launch_deblock(L->out.as<uint8_t>(), 1, n, nz, ny, nx, beta, tc, L->stream), "deblock launch") &&
+        cuda_ok(cudaMemcpyAsync(vol, L->out.p, n, cudaMemcpyDeviceToHost, L->stream), "D2H") && finish(*L, nullptr);
+}
+
 // Blobs in host memory -> voxels in host memory, in groups of chunks.
 // Work items of one host blob whose bytes sit at d_blob on the device: block
 // payloads located through the blob's bitmap and length table

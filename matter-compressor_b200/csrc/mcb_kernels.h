@@ -67,6 +67,10 @@ struct FusedParams {
 int fused_grid(const LaunchCfg &cfg);   // CTAs of k_decode_fused (0: cannot launch)
 cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
+// Deblocking filter in place on `count` dense nz x ny x nx volumes vstride
+// bytes apart (three stream-ordered kernels: x, y, z faces).
+cudaError_t launch_deblock(uint8_t *d_vol, int count, size_t vstride, int nz, int ny, int nx, int beta, int tc,
+                           cudaStream_t s);
 // ---- serving ----
 // One chunk's share of a request: a box of blocks, the request's voxel clip in
 // chunk-local coordinates, and where chunk-local voxel (0,0,0) maps in the output.

@@ -112,6 +112,8 @@ class McLib:
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_plan_config": (None, [vp, vp]),
                 "mc_b200_plan_set_config": (i, [vp, vp]),
+                "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
+                "mc_deblock": (None, [vp, i, i, i, f]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
                 "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
                 "mc_b200_server_open": (vp, [vp, sz, sz, i]),
@@ -177,6 +179,21 @@ class McLib:
         self.L.mc_codec_ctx_free(c)
         self.check()
         return dst
+
+    def deblock(self, vol, quality):
+        """mc_deblock in place on a dense (nz, ny, nx) u8 host volume; returns it."""
+        v = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = v.shape
+        self.L.mc_deblock(_ptr(v), nz, ny, nx, quality)
+        self.check()
+        return v
+
+    def deblock_dev(self, d_vol, count, vol_stride, nz, ny, nx, quality, stream=None):
+        """Deblock `count` dense device volumes in place (mc_b200_deblock_dev)."""
+        rc = self.L.mc_b200_deblock_dev(C.c_void_p(d_vol), count, vol_stride, nz, ny, nx, quality,
+                                        C.c_void_p(stream) if stream else None)
+        self.check()
+        return rc
 
     def set_priors(self, plo, phi):
         if plo is None:

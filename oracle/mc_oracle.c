@@ -762,3 +762,44 @@ void or_decode_chunk(const uint8_t *blob, uint64_t blob_len, uint8_t *out256) {
                    blk + z * 256 + y * 16, 16);
     }
 }
+
+/* ---- decode-side deblocking (src/mc_codec.c:561-595) ----
+ * One face: p1 p0 | q0 q1 along the axis, q0 at index i, the others `step`
+ * apart (src/mc_codec.c:563-574). Air voxels (0) are never touched; a step
+ * across the face as large as beta is a real edge and is kept; otherwise p0
+ * and q0 move towards each other by a clamped 4:1 difference, air neighbours
+ * standing in as their face voxel, and stay inside [1, 255]. */
+static void db_face(uint8_t *v, size_t total, size_t i, size_t step, int beta, int tc) {
+    const int p0 = v[i - step], q0 = v[i];
+    if (p0 == 0 || q0 == 0) return;
+    const int d = q0 - p0;
+    if ((d < 0 ? -d : d) >= beta) return;
+    const int p1 = v[i - 2 * step];
+    const int q1 = i + step < total ? v[i + step] : 0;
+    const int pn = p1 ? p1 : p0, qn = q1 ? q1 : q0;
+    int delta = (4 * d + (pn - qn) + 4) >> 3;   /* arithmetic shift: floor */
+    if (delta > tc) delta = tc;
+    if (delta < -tc) delta = -tc;
+    int a = p0 + delta, b = q0 - delta;
+    a = a < 1 ? 1 : (a > 255 ? 255 : a);
+    b = b < 1 ? 1 : (b > 255 ? 255 : b);
+    v[i - step] = (uint8_t)a;
+    v[i] = (uint8_t)b;
+}
+
+/* Gate and clamp from the quality (src/mc_codec.c:577-578), then the x, y and
+ * z faces in that order (:580-594). */
+void or_deblock(uint8_t *vol, int nz, int ny, int nx, float quality) {
+    const int beta = (int)(3.0f * quality + 6.0f);
+    const int tc = (int)(0.5f * quality + 1.0f);
+    const size_t sy = (size_t)nx, sz = (size_t)ny * (size_t)nx, total = sz * (size_t)nz;
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 16; x < nx; x += 16) db_face(vol, total, z * sz + y * sy + x, 1, beta, tc);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 16; y < ny; y += 16)
+            for (int x = 0; x < nx; ++x) db_face(vol, total, z * sz + y * sy + x, sy, beta, tc);
+    for (int z = 16; z < nz; z += 16)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) db_face(vol, total, z * sz + y * sy + x, sz, beta, tc);
+}

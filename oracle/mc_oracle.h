@@ -70,6 +70,14 @@ void   or_decode_chunk(const uint8_t *blob, uint64_t blob_len, uint8_t *out256);
 void   or_decode_chunk_block(const uint8_t *blob, uint64_t blob_len,
                              int bz, int by, int bx, uint8_t dst[4096]);
 
+/* Decode-side deblocking filter, in place on a dense nz x ny x nx volume
+ * (src/mc_codec.c:561-595, declared at src/matter_compressor.h:106). The
+ * faces between 16-aligned blocks are filtered axis by axis: x, then y, then
+ * z. Neighbours are addressed linearly, as the reference does (a face in the
+ * last voxel of a row reads the next row's first voxel); a read past the end
+ * of the volume, undefined in the reference, reads 0 here. */
+void   or_deblock(uint8_t *vol, int nz, int ny, int nx, float quality);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,7 @@ class Oracle:
             ("or_encode_chunk", sz, [vp, f, f, i, vp, sz]),
             ("or_decode_chunk", None, [vp, u64, vp]),
             ("or_decode_chunk_block", None, [vp, u64, i, i, i, vp]),
+            ("or_deblock", None, [vp, i, i, i, f]),
         ]:
             fn = getattr(L, name)
             fn.restype, fn.argtypes = res, args
@@ -100,6 +101,13 @@ class Oracle:
         a = np.ascontiguousarray(np.frombuffer(blob, np.uint8))
         self.L.or_decode_chunk(_p(a), len(blob), _p(out))
         return out
+
+    def deblock(self, vol, quality):
+        """In-place deblock of a dense (nz, ny, nx) u8 volume; returns it."""
+        v = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = v.shape
+        self.L.or_deblock(_p(v), nz, ny, nx, quality)
+        return v
 
     def priors_for_q(self, q):
         out = np.zeros(256, np.uint16)

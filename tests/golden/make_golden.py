@@ -11,7 +11,11 @@ C API and records inputs, payload bytes and digests of decoded outputs:
   meta.npz     fraction-map coder and XXH64 vectors;
   chunks.npz   whole-chunk blobs from mc_archive_append_chunk_par /
                _ctx (preset ladder), the decoded chunk's digest, and the
-               archive-file digest of a fixed call sequence.
+               archive-file digest of a fixed call sequence;
+  deblock.npz  digests of mc_deblock's output on the shapes.deblock_volumes()
+               inputs over a set of qualities (the volume is followed by a
+               zero plane, so the reference's read past the last z face sees
+               zeros).
 
 Inputs are deterministic integer formulas (shapes.py) so tests regenerate
 them exactly. Usage: python tests/golden/make_golden.py
@@ -150,7 +154,34 @@ def main():
                         blobs=np.concatenate(blobs), decoded_sha=np.array(dsha), archive_sha=np.array(arc_sha),
                         archive_len=np.array(len(data), np.int64))
     print("chunks:", len(blobs), "blobs,", int(boffs[-1]), "bytes; archive", len(data), "bytes")
+    deblock_golden(ref)
+
+
+DEBLOCK_QS = [0.5, 1.0, 3.0, 6.0, 12.0, 40.0]
+
+
+def deblock_golden(ref):
+    import ctypes as C
+    ref.L.mc_deblock.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+    names, qs, digests = [], [], []
+    for name, vol in shapes.deblock_volumes():
+        nz, ny, nx = vol.shape
+        for q in DEBLOCK_QS:
+            buf = np.zeros(vol.size + ny * nx, np.uint8)
+            buf[:vol.size] = vol.ravel()
+            ref.L.mc_deblock(buf.ctypes.data, nz, ny, nx, q)
+            names.append(name)
+            qs.append(q)
+            digests.append(sha(buf[:vol.size]))
+    np.savez_compressed(os.path.join(HERE, "deblock.npz"), names=np.array(names), q=np.array(qs, np.float32),
+                        out_sha=np.array(digests))
+    print("deblock:", len(digests), "cases")
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["deblock"]:
+        r = McLib(REF, b200=False)
+        r.L.mc_codec_init()
+        deblock_golden(r)
+    else:
+        main()

@@ -88,6 +88,26 @@ def archive_sequence():
     ]
 
 
+def deblock_volumes():
+    """(name, volume) pairs for the deblocking filter: blocky volumes whose
+    16-aligned blocks sit at different levels (flat seams that the filter
+    smooths, steep ones it keeps), with air holes and air neighbours, at
+    sizes that are and are not multiples of 16."""
+    out = []
+    for k, (nz, ny, nx) in enumerate([(32, 32, 32), (48, 40, 33), (17, 33, 65), (20, 16, 49), (64, 48, 80)]):
+        z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        blk = (z // 16) * 7 + (y // 16) * 3 + (x // 16) * 5
+        level = 60 + (_hash_u8(blk.ravel(), 10 + k).reshape(blk.shape) % (24 if k % 2 else 120))
+        tex = (x * 3 + y * 5 + z * 7 + k) % 9 - 4
+        vol = level + tex
+        idx = np.arange(vol.size).reshape(vol.shape)
+        vol = np.where(_hash_u8(idx, 20 + k) < 12, 0, vol)                   # speckled air
+        vol = np.where((x + 2 * y + 3 * z + 5 * k) % 97 < 6, 0, vol)         # air sheets
+        vol = np.where(_hash_u8(idx, 30 + k) > 250, 255, vol)                # saturated voxels
+        out.append((f"v{k}_{nz}x{ny}x{nx}", np.clip(vol, 0, 255).astype(np.uint8)))
+    return out
+
+
 def blob_len(data, co):
     """Total length of the chunk blob at file offset co: header, fmap,
     bitmap, one u16 length per present block, payloads."""

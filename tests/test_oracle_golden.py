@@ -1,11 +1,13 @@
 """The oracle (our C restatement) reproduces the reference's golden vectors
 byte for byte: block payloads, decoded blocks, corrupt streams, fraction maps,
 XXH64, whole-chunk blobs and decoded chunks."""
+import os
+
 import numpy as np
 import pytest
 
 import shapes
-from conftest import ctx_q, sha
+from conftest import GOLDEN, ctx_q, sha
 
 
 def test_block_encode_decode(oracle, golden_blocks):
@@ -82,3 +84,13 @@ def test_scan_and_priors(oracle):
     assert oracle.priors_for_q(0.25)[0] == 115  # q <= 1 uses the q=1 table
     mid = oracle.priors_for_q(3.4641)           # log-midpoint lies between
     assert min(lo[0], hi[0]) <= mid[0] <= max(lo[0], hi[0])
+
+
+def test_deblock(oracle):
+    """The deblocking restatement reproduces mc_deblock's output digests."""
+    g = np.load(os.path.join(GOLDEN, "deblock.npz"))
+    vols = dict(shapes.deblock_volumes())
+    for name, q, want in zip(g["names"], g["q"], g["out_sha"]):
+        v = vols[str(name)].copy()
+        oracle.deblock(v, float(q))
+        assert sha(v) == want, (name, q)

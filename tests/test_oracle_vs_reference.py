@@ -33,3 +33,25 @@ def test_garbage_streams(oracle, ref):
         p = rng.integers(0, 256, int(rng.integers(1, 400)), dtype=np.uint8).tobytes()
         q = float([1, 3, 6, 12][t % 4])
         assert np.array_equal(oracle.dec_block(p, q), ref.dec_block(p, q)), t
+
+
+def test_deblock_random_volumes(oracle, ref):
+    """or_deblock == the reference's mc_deblock on seeded blocky volumes of
+    random sizes and qualities (the reference's volume is followed by a zero
+    plane: its read past the last z face then sees what the oracle assumes)."""
+    import ctypes as C
+    ref.L.mc_deblock.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
+    rng = np.random.default_rng(11)
+    for t in range(40):
+        nz, ny, nx = (int(v) for v in rng.integers(1, 70, 3))
+        lv = rng.integers(30, 200, ((nz + 15) // 16, (ny + 15) // 16, (nx + 15) // 16))
+        vol = np.repeat(np.repeat(np.repeat(lv, 16, 0), 16, 1), 16, 2)[:nz, :ny, :nx]
+        vol = vol + rng.integers(-6, 7, vol.shape)
+        vol[rng.random(vol.shape) < 0.05] = 0
+        vol = np.clip(vol, 0, 255).astype(np.uint8)
+        q = float(rng.choice([0.5, 2.0, 6.0, 10.0, 30.0]))
+        buf = np.zeros(vol.size + ny * nx, np.uint8)
+        buf[:vol.size] = vol.ravel()
+        ref.L.mc_deblock(buf.ctypes.data, nz, ny, nx, q)
+        mine = oracle.deblock(vol.copy(), q)
+        assert np.array_equal(mine.ravel(), buf[:vol.size]), (nz, ny, nx, q)
