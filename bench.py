@@ -58,9 +58,10 @@ def parse():
     p.add_argument("--chunks", type=int, default=64)
     p.add_argument("--q", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="decode", choices=["decode", "serve", "regions", "encode", "deblock"],
+    p.add_argument("--workload", default="decode", choices=["decode", "serve", "regions", "encode", "deblock", "pyramid"],
                    help="decode: batched chunk decode (the headline line); serve: request-serving sweep; "
-                        "regions: dataloader region batch; encode: preset-ladder batched encode")
+                        "regions: dataloader region batch; encode: preset-ladder batched encode; "
+                        "deblock: decode-side deblocking of the decoded chunks; pyramid: LOD pyramid build")
     p.add_argument("--rates", default="1000,10000,30000,100000,300000,1000000",
                    help="serve: offered request rates (req/s)")
     p.add_argument("--serve-seconds", type=float, default=0.3, help="serve: arrival window per rate")
@@ -411,8 +412,8 @@ def run_deblock(args):
         e1.record(s)
         torch.cuda.synchronize()
         both.append(e0.elapsed_time(e1))
-    plan.launch(s.cuda_stream)
-    torch.cuda.synchronize()
+    plan.launch(s.cuda_stream)   # dec: decoded voxels again
+    step()                       # out: dec deblocked
     # exactness: the first and last chunk against the oracle's deblock of the same decoded voxels
     from oracle import Oracle
     orc = Oracle()
@@ -474,6 +475,128 @@ def run_deblock(args):
                          "frac": round(achieved / peak, 4), "traffic": None,
                          "algorithmic_bytes_per_launch": 2 * vol},
             "clocks": clk, "cpu_baseline": cpu}
+
+
+def _blob_len(data, co):
+    """Length of the chunk blob at byte offset co of archive bytes."""
+    fml = data[co + 12] | (data[co + 13] << 8)
+    bm = np.frombuffer(data[co + 14 + fml:co + 14 + fml + 512], np.uint8)
+    npres = int(np.unpackbits(bm).sum())
+    lens = np.frombuffer(data[co + 14 + fml + 512:co + 14 + fml + 512 + 2 * npres], np.uint16)
+    return 14 + fml + 512 + 2 * npres + int(lens.astype(np.int64).sum())
+
+
+def _pyramid_levels(nz, ny, nx):
+    """The one-shot builder's LOD loop (src/mc_archive.c:205-220): [(lod, padded extent)]."""
+    d = tuple((n + 255) // 256 * 256 for n in (nz, ny, nx))
+    out = []
+    for lod in range(8):
+        if min(d) < 1 or not (max(d) >= 256 or lod == 0):
+            break
+        out.append((lod, d))
+        if min(v // 2 for v in d) < 1 or (max(v // 2 for v in d) < 256 and lod >= 1):
+            break
+        d = tuple((v + 1) // 2 for v in d)
+    return out
+
+
+def _mc_build(lib_path, vol, q):
+    """The reference's one-shot builder (mc_build) over a host volume, through
+    the oracle's buffer voxel source; returns (archive bytes, seconds)."""
+    import ctypes as C
+    from oracle import ORACLE_LIB
+
+    class Opts(C.Structure):
+        _fields_ = [("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("quality", C.c_float),
+                    ("metadata", C.c_char_p), ("meta_len", C.c_size_t)]
+
+    class Src(C.Structure):
+        _fields_ = [("v", C.c_void_p), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int)]
+    R, O = C.CDLL(lib_path), C.CDLL(ORACLE_LIB)
+    R.mc_codec_init()
+    R.mc_build.restype = C.c_void_p
+    R.mc_build.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    vol = np.ascontiguousarray(vol)
+    nz, ny, nx = vol.shape
+    src, opts, n = Src(vol.ctypes.data, nz, ny, nx), Opts(0, nx, ny, nz, q, None, 0), C.c_size_t()
+    t0 = time.perf_counter()
+    buf = R.mc_build(C.cast(O.or_voxel_source, C.c_void_p), C.byref(src), C.byref(opts), C.byref(n))
+    dt = time.perf_counter() - t0
+    data = C.string_at(buf, n.value)
+    libc.free(buf)
+    return data, dt
+
+
+def run_pyramid(args):
+    """LOD pyramid build: a 1024^3 u8 volume resident in HBM appended with all
+    its LODs (decimated on the device, encoded by the batched encoder, installed
+    in the archive file) by one mc_b200_append_pyramid call per step."""
+    from mcb200 import McLib
+    import volumes
+    lib = McLib.product()
+    dims = (1024, 1024, 1024)
+    vol = volumes.region(7, (0, 0, 0), dims, 0.4, device="cuda").contiguous()
+    td = tempfile.mkdtemp()
+    times, nl, chunks, arc_bytes = [], 0, 0, 0
+    for k in range(args.warmup + args.steps):
+        path = os.path.join(td, f"pyr{k}.mca")
+        with lib.open(path, dims[2], dims[1], dims[0], args.q) as a:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc, nl = a.append_pyramid(vol.data_ptr(), *dims, args.q)
+            dt = time.perf_counter() - t0
+            assert rc == 0
+            arc_bytes = int(a.L.mc_archive_data_len(a.a))
+        os.remove(path)
+        if k >= args.warmup:
+            times.append(dt)
+    s = statistics.median(times)
+    # exactness and the CPU baseline on a 512^3 sample of the same volume: the
+    # device pyramid's chunk blobs against the reference builder's
+    sample = vol[:512, :512, :512].contiguous()
+    h = sample.cpu().numpy()
+    exact, cpu = None, None
+    if not args.no_cpu_baseline:
+        from oracle import REF_FAST_LIB, REF_LIB
+        try:
+            ref_data, _ = _mc_build(REF_LIB, h, args.q)
+            _, cpu_s = _mc_build(REF_FAST_LIB, h, args.q)
+            path = os.path.join(td, "sample.mca")
+            rpath = os.path.join(td, "ref.mca")
+            open(rpath, "wb").write(ref_data)
+            ref = McLib(REF_LIB, b200=False)
+            ref.L.mc_codec_init()
+            exact = True
+            with lib.open(path, 512, 512, 512, args.q) as a, ref.open(rpath, 512, 512, 512, args.q) as ra:
+                assert a.append_pyramid(sample.data_ptr(), 512, 512, 512, args.q)[0] == 0
+                mine = open(path, "rb").read()
+                for lod, (dz, dy, dx) in _pyramid_levels(512, 512, 512):
+                    for c in range(((dz + 255) // 256) * ((dy + 255) // 256) * ((dx + 255) // 256)):
+                        nc = ((dy + 255) // 256, (dx + 255) // 256)
+                        cz, cy, cx = c // (nc[0] * nc[1]), (c // nc[1]) % nc[0], c % nc[1]
+                        o1, o2 = a.chunk_offset(lod, cz, cy, cx), ra.chunk_offset(lod, cz, cy, cx)
+                        b1 = mine[o1:o1 + _blob_len(mine, o1)] if o1 > 1 else b""
+                        b2 = ref_data[o2:o2 + _blob_len(ref_data, o2)] if o2 > 1 else b""
+                        exact &= b1 == b2
+            os.remove(path)
+            os.remove(rpath)
+            cpu = {"value": round(h.size / cpu_s / 1e9, 4), "unit": "GB/s of LOD-0 voxels", "cores": 1,
+                   "kind": "reference",
+                   "sample": "the reference's mc_build (one thread, default-flag build) over a 512^3 sample of the "
+                             "same volume: LOD 0 and LOD 1"}
+        except (FileNotFoundError, OSError) as e:
+            cpu = {"value": None, "sample": f"unavailable: {e}"}
+    os.rmdir(td)
+    vbytes = dims[0] * dims[1] * dims[2]
+    return {"metric": "LOD pyramid build: GB/s of LOD-0 voxels (decimate + encode + install)", "workload": "pyramid",
+            "value": round(vbytes / s / 1e9, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(s * 1e3, 2), "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic", "vs_baseline": None,
+            "config": {"workload": f"mc_b200_append_pyramid of a 1024^3 u8 volume (40 % air) in HBM at q={args.q:g}: "
+                                   f"{nl} LODs into a new archive file per step"},
+            "archive_bytes": arc_bytes, "bit_exact_vs_reference_builder_on_sample": exact, "cpu_baseline": cpu}
 
 
 def run_encode(args):
@@ -697,9 +820,9 @@ def main():
     try:
         if args.workload != "decode":
             if d.world > 1:
-                raise SystemExit("the serve / regions / encode / deblock workloads run on one GPU")
+                raise SystemExit("the serve / regions / encode / deblock / pyramid workloads run on one GPU")
             res = {"serve": run_serve, "regions": run_regions, "encode": run_encode,
-                   "deblock": run_deblock}[args.workload](args)
+                   "deblock": run_deblock, "pyramid": run_pyramid}[args.workload](args)
         else:
             res = run_reference(args, d) if args.impl == "reference" else run_b200(args, d)
         if res is not None:

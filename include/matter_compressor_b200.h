@@ -179,6 +179,22 @@ void mc_b200_plan_free(mc_b200_plan *p);
 int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
                           const mc_u8 *const *vox, int vox_on_device, float q);
 
+/* LOD pyramid on the device. mc_b200_decimate_dev: 2x box decimation of a
+ * dense DEVICE volume nz x ny x nx into d_dst ((nz+1)/2 x (ny+1)/2 x
+ * (nx+1)/2): each output voxel is the rounded mean of its non-zero children,
+ * 0 when all are 0 (src/mc_archive.c:63-72). 0 on success, -1 on bad
+ * arguments or a CUDA error.
+ * mc_b200_append_pyramid: the one-shot builder's pyramid (mc_build,
+ * src/mc_archive.c:184-234) appended to an archive from a dense DEVICE volume:
+ * LOD 0 (the volume zero-padded to whole chunks) and each decimated LOD while
+ * any axis of the current level is at least 256 voxels (LOD 1 always), at
+ * most 8. Chunks are encoded at `quality` (max error 0) with chunk blobs
+ * byte-identical to mc_build's; all-air chunks are left out. *nlods (if
+ * non-NULL) receives the number of levels appended. 0 on success, -1 on an
+ * error (levels appended before it stay in the archive). */
+int mc_b200_decimate_dev(const mc_u8 *d_src, int nz, int ny, int nx, mc_u8 *d_dst, void *stream);
+int mc_b200_append_pyramid(mc_archive *a, const mc_u8 *d_vol, int nz, int ny, int nx, float quality, int *nlods);
+
 /* Serving: block, region and chunk reads of one archive, batched continuously
  * on the GPU behind a decoded-block cache in HBM -- the device-side analogue
  * of the reference's mc_cache read path (src/mc_cache.h). Requests queue on

@@ -647,6 +647,105 @@ int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
     return plan_capture(p) ? 0 : -1;
 }
 
+// ============================================================ LOD pyramid
+int mc_b200_decimate_dev(const mc_u8 *d_src, int nz, int ny, int nx, mc_u8 *d_dst, void *stream) {
+    if (!d_src || !d_dst || nz <= 0 || ny <= 0 || nx <= 0) {
+        set_error("decimate: bad arguments");
+        return -1;
+    }
+    Lane *L = lane();
+    if (!L) return -1;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+    if (!cuda_ok(launch_decimate(d_src, nz, ny, nx, d_dst, s), "decimate launch")) return -1;
+    if (!stream && !finish(*L, nullptr)) return -1;
+    return 0;
+}
+
+// The one-shot builder's pyramid (src/mc_archive.c:184-234) over a device
+// volume: LOD 0 is the volume zero-padded to whole chunks; each next level is
+// the 2x decimation of the previous one while any axis of the current padded
+// extent is at least 256 (LOD 1 always follows LOD 0), at most 8 levels.
+// Decimating the unpadded content gives the padded level's voxels, since a
+// padding child is a zero child. Chunks are gathered 8 at a time; all-air
+// chunks are left out, as the builder leaves them out; the rest are encoded
+// and installed by the batched ctx append.
+int mc_b200_append_pyramid(mc_archive *a, const mc_u8 *d_vol, int nz, int ny, int nx, float quality, int *nlods) {
+    if (nlods) *nlods = 0;
+    if (!a || !d_vol || nz <= 0 || ny <= 0 || nx <= 0) {
+        set_error("append_pyramid: bad arguments");
+        return -1;
+    }
+    Lane *L = lane();
+    if (!L) return -1;
+    constexpr int G = 8;
+    auto pad = [](int n) { return (int)(((int64_t)n + 255) / 256 * 256); };
+    int pd[3] = {pad(nz), pad(ny), pad(nx)};   // padded extent of the current level
+    int cd[3] = {nz, ny, nx};                  // its non-padding content
+    const size_t lod1 = (size_t)((nz + 1) / 2) * ((ny + 1) / 2) * ((nx + 1) / 2);
+    const size_t lod2 = (size_t)((nz + 3) / 4) * ((ny + 3) / 4) * ((nx + 3) / 4);
+    if (!L->pyr_stage.ensure(kChunkBytes * G) || !L->pyr_flag.ensure(sizeof(uint32_t) * G) ||
+        !L->pyr_a.ensure(lod1) || !L->pyr_b.ensure(lod2 ? lod2 : 1))
+        return -1;
+    mc_codec_ctx *C = mc_codec_ctx_new();
+    if (!C) {
+        set_error("append_pyramid: out of memory");
+        return -1;
+    }
+    mc_codec_ctx_set_quality(C, quality);
+    const uint8_t *cur = d_vol;
+    int done = 0, rc = 0;
+    for (int lod = 0; lod < 8 && rc == 0; ++lod) {
+        const int mn = std::min(pd[0], std::min(pd[1], pd[2])), mx = std::max(pd[0], std::max(pd[1], pd[2]));
+        if (mn < 1 || !(mx >= 256 || lod == 0)) break;
+        const int nc[3] = {(pd[0] + 255) / 256, (pd[1] + 255) / 256, (pd[2] + 255) / 256};
+        const int total = nc[0] * nc[1] * nc[2];
+        for (int c0 = 0; c0 < total && rc == 0; c0 += G) {
+            const int g = std::min(G, total - c0);
+            uint32_t flags[G] = {0};
+            bool ok = cuda_ok(cudaMemsetAsync(L->pyr_flag.p, 0, sizeof(uint32_t) * G, L->stream), "memset");
+            for (int j = 0; j < g && ok; ++j) {
+                const int c = c0 + j, cz = c / (nc[1] * nc[2]), cy = (c / nc[2]) % nc[1], cx = c % nc[2];
+                ok = cuda_ok(launch_gather_chunk(cur, cd[0], cd[1], cd[2], cz, cy, cx,
+                                                 L->pyr_stage.as<uint8_t>() + kChunkBytes * j,
+                                                 L->pyr_flag.as<uint32_t>() + j, L->stream),
+                             "gather launch");
+            }
+            ok = ok && cuda_ok(cudaMemcpyAsync(flags, L->pyr_flag.p, sizeof(uint32_t) * G, cudaMemcpyDeviceToHost,
+                                               L->stream), "D2H flags") &&
+                 finish(*L, nullptr);
+            if (!ok) { rc = -1; break; }
+            std::vector<int> coords;
+            std::vector<const mc_u8 *> ptrs;
+            for (int j = 0; j < g; ++j) {
+                if (!flags[j]) continue;   // all air: left out
+                const int c = c0 + j;
+                coords.insert(coords.end(), {c / (nc[1] * nc[2]), (c / nc[2]) % nc[1], c % nc[2]});
+                ptrs.push_back(L->pyr_stage.as<uint8_t>() + kChunkBytes * j);
+            }
+            if (!ptrs.empty() &&
+                mc_b200_append_chunks(a, C, lod, coords.data(), (int)ptrs.size(), ptrs.data(), 1, quality) != 0)
+                rc = -1;
+        }
+        if (rc) break;
+        done = lod + 1;
+        if (mn / 2 < 1) break;
+        if (mx / 2 < 256 && lod >= 1) break;
+        uint8_t *next = (lod & 1) ? L->pyr_b.as<uint8_t>() : L->pyr_a.as<uint8_t>();
+        if (!cuda_ok(launch_decimate(cur, cd[0], cd[1], cd[2], next, L->stream), "decimate launch")) {
+            rc = -1;
+            break;
+        }
+        cur = next;
+        for (int k = 0; k < 3; ++k) {
+            cd[k] = (cd[k] + 1) / 2;
+            pd[k] = (pd[k] + 1) / 2;
+        }
+    }
+    mc_codec_ctx_free(C);
+    if (nlods) *nlods = done;
+    return rc;
+}
+
 void mc_b200_plan_free(mc_b200_plan *p) {
     if (!p) return;
     if (p->exec) cudaGraphExecDestroy(p->exec);

@@ -69,6 +69,12 @@ cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
 // Deblocking filter in place on `count` dense nz x ny x nx volumes vstride
 // bytes apart (three stream-ordered kernels: x, y, z faces).
+// LOD pyramid: 2x decimation of a dense dz x dy x dx volume into
+// ((dz+1)/2, (dy+1)/2, (dx+1)/2), and the gather of chunk (cz, cy, cx) of a
+// dense volume into a 256^3 buffer (zeros outside; *d_any |= 1 if non-zero).
+cudaError_t launch_decimate(const uint8_t *d_src, int dz, int dy, int dx, uint8_t *d_dst, cudaStream_t s);
+cudaError_t launch_gather_chunk(const uint8_t *d_src, int nz, int ny, int nx, int cz, int cy, int cx, uint8_t *d_dst,
+                                uint32_t *d_any, cudaStream_t s);
 cudaError_t launch_deblock(uint8_t *d_vol, int count, size_t vstride, int nz, int ny, int nx, int beta, int tc,
                            cudaStream_t s);
 // ---- serving ----

@@ -98,6 +98,7 @@ struct Lane {
     DecodeBatch batch;
     DevBuf enc_items, enc_len, enc_frac, enc_pay, src;
     DevBuf b_scratch, b_lens16, b_bitmap, b_fmap, b_fml, b_np, b_len, b_off, b_q, blobs;
+    DevBuf pyr_stage, pyr_a, pyr_b, pyr_flag;   // LOD pyramid: chunk staging, level volumes, all-air flags
     HostBuf h_items, h_base, h_stage, h_misc;
     LaunchCfg cfg;
     BlobSlot pipe[2];

@@ -113,6 +113,8 @@ class McLib:
                 "mc_b200_plan_config": (None, [vp, vp]),
                 "mc_b200_plan_set_config": (i, [vp, vp]),
                 "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
+                "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
+                "mc_b200_append_pyramid": (i, [vp, vp, i, i, i, f, C.POINTER(i)]),
                 "mc_deblock": (None, [vp, i, i, i, f]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
                 "mc_b200_decode_blocks_noalloc": (i, [vp, vp, i, f, vp, vp]),
@@ -192,6 +194,13 @@ class McLib:
         """Deblock `count` dense device volumes in place (mc_b200_deblock_dev)."""
         rc = self.L.mc_b200_deblock_dev(C.c_void_p(d_vol), count, vol_stride, nz, ny, nx, quality,
                                         C.c_void_p(stream) if stream else None)
+        self.check()
+        return rc
+
+    def decimate_dev(self, d_src, nz, ny, nx, d_dst, stream=None):
+        """2x LOD decimation of a dense device volume (mc_b200_decimate_dev)."""
+        rc = self.L.mc_b200_decimate_dev(C.c_void_p(d_src), nz, ny, nx, C.c_void_p(d_dst),
+                                         C.c_void_p(stream) if stream else None)
         self.check()
         return rc
 
@@ -308,6 +317,13 @@ class Archive:
             self.L.mc_codec_ctx_free(c)
         self.lib.check()
         return rc
+
+    def append_pyramid(self, d_vol, nz, ny, nx, q):
+        """mc_b200_append_pyramid: every LOD of a dense device volume; returns (rc, levels)."""
+        n = C.c_int()
+        rc = self.L.mc_b200_append_pyramid(self.a, C.c_void_p(d_vol), nz, ny, nx, q, C.byref(n))
+        self.lib.check()
+        return rc, n.value
 
     def sync_device(self):
         base = C.c_void_p()

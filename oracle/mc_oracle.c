@@ -803,3 +803,26 @@ void or_deblock(uint8_t *vol, int nz, int ny, int nx, float quality) {
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) db_face(vol, total, z * sz + y * sy + x, sz, beta, tc);
 }
+
+/* ---- LOD decimation (src/mc_archive.c:63-72) ---- */
+void or_decimate(const uint8_t *src, int DZ, int DY, int DX, uint8_t *dst) {
+    const int hz = (DZ + 1) / 2, hy = (DY + 1) / 2, hx = (DX + 1) / 2;
+    for (int z = 0; z < hz; ++z)
+        for (int y = 0; y < hy; ++y)
+            for (int x = 0; x < hx; ++x) {
+                int sum = 0, n = 0;
+                for (int c = 0; c < 8; ++c) {
+                    const int sz = 2 * z + (c >> 2), sy = 2 * y + ((c >> 1) & 1), sx = 2 * x + (c & 1);
+                    if (sz >= DZ || sy >= DY || sx >= DX) continue;
+                    const int v = src[((size_t)sz * DY + sy) * DX + sx];
+                    if (v) { sum += v; n++; }
+                }
+                dst[((size_t)z * hy + y) * hx + x] = n ? (uint8_t)((sum + n / 2) / n) : 0;
+            }
+}
+
+uint8_t or_voxel_source(void *ud, int x, int y, int z) {
+    const or_volume_src *s = (const or_volume_src *)ud;
+    if ((unsigned)z >= (unsigned)s->nz || (unsigned)y >= (unsigned)s->ny || (unsigned)x >= (unsigned)s->nx) return 0;
+    return s->v[((size_t)z * s->ny + y) * s->nx + x];
+}

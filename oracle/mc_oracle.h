@@ -78,6 +78,18 @@ void   or_decode_chunk_block(const uint8_t *blob, uint64_t blob_len,
  * of the volume, undefined in the reference, reads 0 here. */
 void   or_deblock(uint8_t *vol, int nz, int ny, int nx, float quality);
 
+/* 2x LOD decimation (src/mc_archive.c:63-72): output voxel (z,y,x) of a
+ * ((DZ+1)/2, (DY+1)/2, (DX+1)/2) volume is the rounded mean of the NON-ZERO
+ * voxels among its up to 8 children (children past an odd edge do not
+ * exist), or 0 when all children are 0. */
+void   or_decimate(const uint8_t *src, int DZ, int DY, int DX, uint8_t *dst);
+
+/* A voxel source over a dense buffer for the reference's one-shot builder
+ * (mc_voxel_fn, src/matter_compressor.h:134): ud points to an
+ * or_volume_src; voxels outside the buffer read 0. */
+typedef struct { const uint8_t *v; int nz, ny, nx; } or_volume_src;
+uint8_t or_voxel_source(void *ud, int x, int y, int z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,7 @@ class Oracle:
             ("or_decode_chunk", None, [vp, u64, vp]),
             ("or_decode_chunk_block", None, [vp, u64, i, i, i, vp]),
             ("or_deblock", None, [vp, i, i, i, f]),
+            ("or_decimate", None, [vp, i, i, i, vp]),
         ]:
             fn = getattr(L, name)
             fn.restype, fn.argtypes = res, args
@@ -108,6 +109,14 @@ class Oracle:
         nz, ny, nx = v.shape
         self.L.or_deblock(_p(v), nz, ny, nx, quality)
         return v
+
+    def decimate(self, vol):
+        """2x LOD decimation of a dense (DZ, DY, DX) u8 volume."""
+        v = np.ascontiguousarray(vol, np.uint8)
+        dz, dy, dx = v.shape
+        out = np.zeros(((dz + 1) // 2, (dy + 1) // 2, (dx + 1) // 2), np.uint8)
+        self.L.or_decimate(_p(v), dz, dy, dx, _p(out))
+        return out
 
     def priors_for_q(self, q):
         out = np.zeros(256, np.uint16)

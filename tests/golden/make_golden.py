@@ -12,6 +12,9 @@ C API and records inputs, payload bytes and digests of decoded outputs:
   chunks.npz   whole-chunk blobs from mc_archive_append_chunk_par /
                _ctx (preset ladder), the decoded chunk's digest, and the
                archive-file digest of a fixed call sequence;
+  pyramid.npz  mc_build (the one-shot builder, which box-decimates LODs) on
+               shapes.pyramid_volume() at two qualities: the digest of every
+               LOD's chunk blobs, keyed by (q, lod, cz, cy, cx);
   deblock.npz  digests of mc_deblock's output on the shapes.deblock_volumes()
                inputs over a set of qualities (the volume is followed by a
                zero plane, so the reference's read past the last z face sees
@@ -155,6 +158,54 @@ def main():
                         archive_len=np.array(len(data), np.int64))
     print("chunks:", len(blobs), "blobs,", int(boffs[-1]), "bytes; archive", len(data), "bytes")
     deblock_golden(ref)
+    pyramid_golden(ref)
+
+
+PYRAMID_QS = [6.0, 0.25]
+
+
+def pyramid_golden(ref):
+    import ctypes as C
+
+    class Opts(C.Structure):
+        _fields_ = [("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("quality", C.c_float),
+                    ("metadata", C.c_char_p), ("meta_len", C.c_size_t)]
+
+    class Src(C.Structure):
+        _fields_ = [("v", C.c_void_p), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int)]
+
+    orc = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    vol = shapes.pyramid_volume()
+    nz, ny, nx = vol.shape
+    src = Src(vol.ctypes.data, nz, ny, nx)
+    ref.L.mc_build.restype = C.c_void_p
+    ref.L.mc_build.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    keys, digests = [], []
+    levels = shapes.pyramid_levels(nz, ny, nx)
+    for q in PYRAMID_QS:
+        opts = Opts(0, nx, ny, nz, q, None, 0)
+        n = C.c_size_t()
+        buf = ref.L.mc_build(C.cast(orc.or_voxel_source, C.c_void_p), C.byref(src), C.byref(opts), C.byref(n))
+        data = C.string_at(buf, n.value)
+        libc.free(buf)
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "p.mca")
+            open(path, "wb").write(data)
+            with ref.open(path, nx, ny, nz, q) as a:
+                for lod, (dz, dy, dx) in levels:
+                    for cz in range((dz + 255) // 256):
+                        for cy in range((dy + 255) // 256):
+                            for cx in range((dx + 255) // 256):
+                                co = a.chunk_offset(lod, cz, cy, cx)
+                                if co <= 1:
+                                    continue
+                                keys.append((q, lod, cz, cy, cx))
+                                digests.append(hashlib.sha256(data[co:co + shapes.blob_len(data, co)]).hexdigest())
+    np.savez_compressed(os.path.join(HERE, "pyramid.npz"), keys=np.array(keys, np.float64), blob_sha=np.array(digests),
+                        levels=np.array([lv for lv, _ in levels], np.int32))
+    print("pyramid:", len(digests), "blobs over", len(levels), "LODs")
 
 
 DEBLOCK_QS = [0.5, 1.0, 3.0, 6.0, 12.0, 40.0]
@@ -179,9 +230,9 @@ def deblock_golden(ref):
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["deblock"]:
+    if sys.argv[1:] in (["deblock"], ["pyramid"]):
         r = McLib(REF, b200=False)
         r.L.mc_codec_init()
-        deblock_golden(r)
+        (deblock_golden if sys.argv[1] == "deblock" else pyramid_golden)(r)
     else:
         main()

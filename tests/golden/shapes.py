@@ -108,6 +108,63 @@ def deblock_volumes():
     return out
 
 
+def pyramid_volume():
+    """A 150 x 200 x 1100 (z, y, x) volume for the LOD pyramid: padded to
+    256 x 256 x 1280 it has 5 LOD-0 chunks (one all air), 3 at LOD 1 and 2 at
+    LOD 2; material with air holes, odd extents on every axis."""
+    nz, ny, nx = 150, 200, 1100
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    idx = (z * ny + y) * nx + x
+    vol = 40 + ((x * x // 97 + y * 3 + z * 5) % 150) + _hash_u8(idx.ravel(), 7).reshape(idx.shape) % 9
+    vol = np.where(((x // 96) + (y // 64) + (z // 48)) % 5 == 0, 0, vol)      # air pockets
+    vol = np.where((x >= 768) & (x < 1024), 0, vol)                           # one all-air LOD-0 chunk
+    vol = np.where(_hash_u8(idx.ravel(), 8).reshape(idx.shape) < 20, 0, vol)  # speckled air
+    return vol.astype(np.uint8)
+
+
+def pyramid_levels(nz, ny, nx):
+    """The reference one-shot builder's LOD loop (src/mc_archive.c:205-220):
+    [(lod, (dz, dy, dx))] with the padded extent of each level. LOD 0 is the
+    volume padded to multiples of 256; each next level halves (rounding up)
+    while any axis of the current level is at least 256 (LOD 1 always
+    follows LOD 0), at most 8 levels."""
+    pad = lambda n: (n + 255) // 256 * 256
+    d = (pad(nz), pad(ny), pad(nx))
+    out = []
+    for lod in range(8):
+        if min(d) < 1 or not (max(d) >= 256 or lod == 0):
+            break
+        out.append((lod, d))
+        if min(v // 2 for v in d) < 1:
+            break
+        if max(v // 2 for v in d) < 256 and lod >= 1:
+            break
+        d = tuple((v + 1) // 2 for v in d)
+    return out
+
+
+def pyramid_chunks(vol, decimate):
+    """{(lod, cz, cy, cx): 256^3 chunk} of every LOD of the builder's pyramid
+    over `vol`, using `decimate` for the 2x steps; all-air chunks left out."""
+    levels = pyramid_levels(*vol.shape)
+    cur = np.zeros(levels[0][1], np.uint8)
+    cur[:vol.shape[0], :vol.shape[1], :vol.shape[2]] = vol
+    out = {}
+    for i, (lod, (dz, dy, dx)) in enumerate(levels):
+        assert cur.shape == (dz, dy, dx)
+        for cz in range((dz + 255) // 256):
+            for cy in range((dy + 255) // 256):
+                for cx in range((dx + 255) // 256):
+                    c = np.zeros((256, 256, 256), np.uint8)
+                    part = cur[cz * 256:cz * 256 + 256, cy * 256:cy * 256 + 256, cx * 256:cx * 256 + 256]
+                    c[:part.shape[0], :part.shape[1], :part.shape[2]] = part
+                    if c.any():
+                        out[(lod, cz, cy, cx)] = c
+        if i + 1 < len(levels):
+            cur = decimate(cur)
+    return out
+
+
 def blob_len(data, co):
     """Total length of the chunk blob at file offset co: header, fmap,
     bitmap, one u16 length per present block, payloads."""

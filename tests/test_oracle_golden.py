@@ -94,3 +94,17 @@ def test_deblock(oracle):
         v = vols[str(name)].copy()
         oracle.deblock(v, float(q))
         assert sha(v) == want, (name, q)
+
+
+def test_pyramid(oracle):
+    """The one-shot builder's LOD pyramid restated with or_decimate and the
+    oracle's chunk encoder: every LOD's chunk blobs == mc_build's digests."""
+    import hashlib
+    g = np.load(os.path.join(GOLDEN, "pyramid.npz"))
+    chunks = shapes.pyramid_chunks(shapes.pyramid_volume(), oracle.decimate)
+    for q in sorted(set(float(k[0]) for k in g["keys"])):
+        want = {tuple(int(v) for v in k[1:]): d for k, d in zip(g["keys"], g["blob_sha"]) if float(k[0]) == q}
+        assert set(want) == set(chunks), q
+        for key, c in chunks.items():
+            blob = oracle.encode_chunk(c.reshape(-1), q, 0, header_q=q)
+            assert hashlib.sha256(blob).hexdigest() == want[key], (q, key)
