@@ -322,6 +322,18 @@ def run_regions(args):
     host_ms = (time.perf_counter() - t0) * 1e3
     exact = bool(all(np.array_equal(dev[i * stride:i * stride + crop], host[i * stride:i * stride + crop])
                      for i in range(len(boxes))))
+    # archive verification: chained XXH64 of every chunk blob of every LOD,
+    # hashed on the device from the HBM mirror (the host walks the node tables)
+    _, base, alen = a.sync_device()
+    arc = np.fromfile(path, np.uint8)
+    vt = []
+    for _ in range(max(3, args.steps)):
+        t0 = time.perf_counter()
+        vbad = lib.L.mc_b200_verify_archive_dev(arc.ctypes.data, base, alen, 0)
+        vt.append(time.perf_counter() - t0)
+    verify = {"api": "mc_b200_verify_archive_dev", "archive_bytes": int(alen), "corrupt": int(vbad),
+              "ms": round(statistics.median(vt[1:]) * 1e3, 3),
+              "gbs": round(alen / statistics.median(vt[1:]) / 1e9, 3)}
     a.close()
     # parity against the reference's strict build (its default fast-math build
     # differs from itself under other flags by +-1 on about 1e-6 of voxels);
@@ -338,6 +350,11 @@ def run_regions(args):
                     rout = ra.read_regions(0, boxes, 128, 128, 128, batch_stride=stride)
                     ref_s = time.perf_counter() - t0
                 if timed:
+                    t0 = time.perf_counter()
+                    rbad = ref.L.mc_verify_archive(arc.ctypes.data, arc.size, 0)
+                    verify["reference_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+                    verify["reference_corrupt"] = int(rbad)
+                    verify["reference_api"] = "mc_verify_archive (one thread, the reference's default-flag build)"
                     cpu = {"value": round(len(boxes) * crop / ref_s / 1e9, 4), "unit": "GB/s",
                            "cores": min(os.cpu_count() or 4, 16), "kind": "reference",
                            "sample": "one mc_archive_read_regions(nthreads=0) call over the same 64 boxes, "
@@ -359,6 +376,7 @@ def run_regions(args):
             "bit_exact_device_vs_host_call": exact, "bit_exact_vs_reference_strict_build": exact_ref,
             "plain_host_call": {"api": "mc_archive_read_regions (host output)", "ms": round(host_ms, 3),
                                 "gbs": round(gb / (host_ms / 1e3), 3)},
+            "verify": verify,
             "cpu_baseline": cpu}
 
 

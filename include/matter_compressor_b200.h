@@ -179,6 +179,14 @@ void mc_b200_plan_free(mc_b200_plan *p);
 int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *coords, int n,
                           const mc_u8 *const *vox, int vox_on_device, float q);
 
+/* mc_verify_archive with the hashing on the device: the archive's bytes in
+ * HOST memory (arc, for the walk over its node tables) and the same bytes in
+ * DEVICE memory (d_arc, e.g. the mirror from mc_b200_archive_sync), len bytes
+ * each. Every chunk blob's chained XXH64 is recomputed on the GPU and
+ * compared with the stored one. Returns the number of corrupt node tables and
+ * blobs, like mc_verify_archive (src/matter_compressor.h:370), or -1. */
+long mc_b200_verify_archive_dev(const uint8_t *arc, const uint8_t *d_arc, size_t len, int verbose);
+
 /* LOD pyramid on the device. mc_b200_decimate_dev: 2x box decimation of a
  * dense DEVICE volume nz x ny x nx into d_dst ((nz+1)/2 x (ny+1)/2 x
  * (nx+1)/2): each output voxel is the rounded mean of its non-zero children,

@@ -647,6 +647,44 @@ int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
     return plan_capture(p) ? 0 : -1;
 }
 
+// ============================================================ device verify
+long mc_b200_verify_archive_dev(const uint8_t *arc, const uint8_t *d_arc, size_t len, int verbose) {
+    if (!arc || !d_arc) {
+        set_error("verify: bad arguments");
+        return -1;
+    }
+    std::vector<VerifyBlob> blobs;
+    long total = 0;
+    long bad = verify_walk(arc, len, blobs, &total);
+    if (bad < 0) return -1;
+    const int n = (int)blobs.size();
+    if (n) {
+        Lane *L = lane();
+        if (!L) return -1;
+        std::vector<VerifyItem> items((size_t)n);
+        for (int i = 0; i < n; ++i) items[i] = VerifyItem{blobs[i].co, blobs[i].len, blobs[i].np, 0};
+        std::vector<uint32_t> flags((size_t)n);
+        if (!L->ver_items.ensure(sizeof(VerifyItem) * (size_t)n) || !L->ver_bad.ensure(sizeof(uint32_t) * (size_t)n) ||
+            !cuda_ok(cudaMemcpyAsync(L->ver_items.p, items.data(), sizeof(VerifyItem) * (size_t)n,
+                                     cudaMemcpyHostToDevice, L->stream), "H2D verify items") ||
+            !cuda_ok(launch_verify_hash(d_arc, len, L->ver_items.as<VerifyItem>(), n, L->ver_bad.as<uint32_t>(),
+                                        L->stream), "verify launch") ||
+            !cuda_ok(cudaMemcpyAsync(flags.data(), L->ver_bad.p, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost,
+                                     L->stream), "D2H verify flags") ||
+            !finish(*L, nullptr))
+            return -1;
+        for (int i = 0; i < n; ++i) {
+            if (!flags[i]) continue;
+            bad++;
+            if (verbose)
+                fprintf(stderr, "mc_verify: lod %d node %d/%d/%d chunk@%llu CORRUPT\n", blobs[i].lod, blobs[i].n2,
+                        blobs[i].n1, blobs[i].n0, (unsigned long long)blobs[i].co);
+        }
+    }
+    if (verbose) fprintf(stderr, "mc_verify: %ld chunks checked, %ld corrupt\n", total, bad);
+    return bad;
+}
+
 // ============================================================ LOD pyramid
 int mc_b200_decimate_dev(const mc_u8 *d_src, int nz, int ny, int nx, mc_u8 *d_dst, void *stream) {
     if (!d_src || !d_dst || nz <= 0 || ny <= 0 || nx <= 0) {

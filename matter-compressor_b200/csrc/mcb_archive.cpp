@@ -295,6 +295,61 @@ uint8_t *mirror_sync(mc_archive *a, Lane &L) {
 }  // namespace mcb
 
 // ================================================================= codec ctx
+namespace mcb {
+
+// The node walk of src/mc_archive.c:1072-1111 with its bounds: every header-
+// derived offset is checked against [kHdr, len) before it is read, and a
+// blob's structure (header, fmap, bitmap, length table, payloads) must lie
+// inside the archive (src/mc_archive.h:212-226). Node tables and blobs that
+// fail count as bad; the blobs that pass are appended to `out` for hashing.
+long verify_walk(const uint8_t *arc, size_t len, std::vector<VerifyBlob> &out, long *total) {
+    *total = 0;
+    if (!arc || len < kHdr) return -1;
+    auto node_ok = [len](uint64_t off) { return off >= kHdr && off <= len && len - off >= kNodeBytes; };
+    long bad = 0;
+    for (int lod = 0; lod < 8; ++lod) {
+        uint64_t root = rd64(arc + HROOT + (uint64_t)lod * 8);
+        if (!root) continue;
+        if (!node_ok(root)) { bad++; continue; }
+        for (int n2 = 0; n2 < kGrid3; ++n2) {
+            uint64_t inner = rd64(arc + root + (uint64_t)n2 * 8);
+            if (!inner) continue;
+            if (!node_ok(inner)) { bad++; continue; }
+            for (int n1 = 0; n1 < kGrid3; ++n1) {
+                uint64_t shard = rd64(arc + inner + (uint64_t)n1 * 8);
+                if (!shard) continue;
+                if (!node_ok(shard)) { bad++; continue; }
+                for (int n0 = 0; n0 < kGrid3; ++n0) {
+                    uint64_t co = rd64(arc + shard + (uint64_t)n0 * 8);
+                    if (co <= kSlotZero) continue;
+                    (*total)++;
+                    if (co > len || len - co < (uint64_t)kBlobHdr) { bad++; continue; }
+                    uint16_t fml;
+                    memcpy(&fml, arc + co + 12, 2);
+                    const uint64_t bm_off = co + kBlobHdr + fml;
+                    if (bm_off > len || len - bm_off < (uint64_t)kBitmapBytes) { bad++; continue; }
+                    uint32_t np = 0;
+                    for (int i = 0; i < kBitmapBytes; ++i) np += (uint32_t)__builtin_popcount(arc[bm_off + i]);
+                    const uint64_t lens_off = bm_off + kBitmapBytes;
+                    if (len - lens_off < 2ull * np) { bad++; continue; }
+                    uint64_t pay = 0;
+                    for (uint32_t k = 0; k < np; ++k) {
+                        uint16_t l;
+                        memcpy(&l, arc + lens_off + 2 * k, 2);
+                        pay += l;
+                    }
+                    const uint64_t bl = lens_off + 2ull * np + pay - co;
+                    if (co + bl > len) { bad++; continue; }
+                    out.push_back(VerifyBlob{co, bl, np, lod, n2, n1, n0});
+                }
+            }
+        }
+    }
+    return bad;
+}
+
+}  // namespace mcb
+
 extern "C" {
 
 mc_codec_ctx *mc_codec_ctx_new(void) { return new (std::nothrow) mc_codec_ctx(); }
@@ -654,51 +709,16 @@ int mc_archive_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count, lo
 
 // src/mc_archive.c:1072-1111: walk every chunk of every LOD, recompute its hash
 long mc_verify_archive(const uint8_t *arc, size_t len, int verbose) {
-    if (!arc || len < kHdr) return -1;
-    auto node_ok = [len](uint64_t off) { return off >= kHdr && off <= len && len - off >= kNodeBytes; };
-    auto blob_ok = [arc, len](uint64_t co) -> uint64_t {   // src/mc_archive.h:212-226
-        if (co > len || len - co < (uint64_t)kBlobHdr) return 0;
-        uint16_t fml;
-        memcpy(&fml, arc + co + 12, 2);
-        uint64_t bm_off = co + kBlobHdr + fml;
-        if (bm_off > len || len - bm_off < (uint64_t)kBitmapBytes) return 0;
-        uint32_t np = 0;
-        for (int i = 0; i < kBitmapBytes; ++i) np += (uint32_t)__builtin_popcount(arc[bm_off + i]);
-        uint64_t lens_off = bm_off + kBitmapBytes;
-        if (len - lens_off < 2ull * np) return 0;
-        uint64_t pay = 0;
-        for (uint32_t s = 0; s < np; ++s) { uint16_t l; memcpy(&l, arc + lens_off + 2 * s, 2); pay += l; }
-        uint64_t total = lens_off + 2ull * np + pay - co;
-        if (co + total > len) return 0;
-        return total;
-    };
-    long bad = 0, total = 0;
-    for (int lod = 0; lod < 8; ++lod) {
-        uint64_t root = rd64(arc + HROOT + (uint64_t)lod * 8);
-        if (!root) continue;
-        if (!node_ok(root)) { bad++; continue; }
-        for (int n2 = 0; n2 < kGrid3; ++n2) {
-            uint64_t inner = rd64(arc + root + (uint64_t)n2 * 8);
-            if (!inner) continue;
-            if (!node_ok(inner)) { bad++; continue; }
-            for (int n1 = 0; n1 < kGrid3; ++n1) {
-                uint64_t shard = rd64(arc + inner + (uint64_t)n1 * 8);
-                if (!shard) continue;
-                if (!node_ok(shard)) { bad++; continue; }
-                for (int n0 = 0; n0 < kGrid3; ++n0) {
-                    uint64_t co = rd64(arc + shard + (uint64_t)n0 * 8);
-                    if (co <= kSlotZero) continue;
-                    total++;
-                    uint64_t bl = blob_ok(co);
-                    if (!bl) { bad++; continue; }
-                    if (rd64(arc + co + 4) != host_blob_hash(arc + co, bl)) {
-                        bad++;
-                        if (verbose)
-                            fprintf(stderr, "mc_verify: lod %d node %d/%d/%d chunk@%llu CORRUPT\n", lod, n2, n1, n0,
-                                    (unsigned long long)co);
-                    }
-                }
-            }
+    std::vector<VerifyBlob> blobs;
+    long total = 0;
+    long bad = verify_walk(arc, len, blobs, &total);
+    if (bad < 0) return -1;
+    for (const VerifyBlob &v : blobs) {
+        if (rd64(arc + v.co + 4) != host_blob_hash(arc + v.co, v.len)) {
+            bad++;
+            if (verbose)
+                fprintf(stderr, "mc_verify: lod %d node %d/%d/%d chunk@%llu CORRUPT\n", v.lod, v.n2, v.n1, v.n0,
+                        (unsigned long long)v.co);
         }
     }
     if (verbose) fprintf(stderr, "mc_verify: %ld chunks checked, %ld corrupt\n", total, bad);

@@ -52,5 +52,14 @@ int install_blob(mc_archive *a, int lod, int cz, int cy, int cx, const uint8_t *
 int mark_zero(mc_archive *a, int lod, int cz, int cy, int cx);
 // Bring the HBM mirror up to date and order the lane's stream after it.
 uint8_t *mirror_sync(mc_archive *a, Lane &L);
+// A chunk blob that passed the structural checks of the verify walk.
+struct VerifyBlob {
+    uint64_t co, len;       // blob offset and length in the archive
+    uint32_t np;            // present blocks (bitmap popcount)
+    int lod, n2, n1, n0;    // where the walk found it
+};
+// The mc_verify_archive node walk: -1 if the header is unusable, else the
+// number of node tables and blobs that fail their bounds; the rest go to out.
+long verify_walk(const uint8_t *arc, size_t len, std::vector<VerifyBlob> &out, long *total);
 
 }  // namespace mcb

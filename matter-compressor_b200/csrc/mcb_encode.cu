@@ -462,17 +462,40 @@ __device__ __forceinline__ uint32_t ld32u(const uint8_t *p) {
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
 
+// Stripe loaders: bytes one at a time (any address), or two aligned 64-bit
+// loads joined by a funnel shift when both words lie below `limit`.
+struct ByteLoad {
+    __device__ uint64_t operator()(const uint8_t *p) const { return ld64u(p); }
+};
+struct FunnelLoad {
+    const uint8_t *limit;
+    __device__ uint64_t operator()(const uint8_t *p) const {
+        const uint32_t a = (uint32_t)((uintptr_t)p & 7);
+        const uint64_t *w = reinterpret_cast<const uint64_t *>(p - a);
+        if (reinterpret_cast<const uint8_t *>(w + 2) > limit) return ld64u(p);
+        const uint64_t lo = __ldg(w), hi = __ldg(w + 1);
+        return a ? (lo >> (8 * a)) | (hi << (64 - 8 * a)) : lo;
+    }
+};
+
 // XXH64 computed by 4 cooperating lanes (lanes 0..3 of a warp): lane i owns
 // accumulator i over the 32-byte stripes; lane 0 merges and hashes the tail.
 // Returns the hash in every participating lane.
-__device__ uint64_t xxh64_4(const uint8_t *p, uint64_t len, uint64_t seed, int lane, unsigned gm) {
+template <class LD = ByteLoad>
+__device__ uint64_t xxh64_4(const uint8_t *p, uint64_t len, uint64_t seed, int lane, unsigned gm, LD ld = LD()) {
     uint64_t h = 0;
     const uint64_t nstripes = len >= 32 ? len / 32 : 0;
     uint64_t acc = 0;
     if (nstripes) {
         acc = lane == 0 ? seed + XP1 + XP2 : lane == 1 ? seed + XP2 : lane == 2 ? seed : seed - XP1;
         const uint8_t *q = p + 8 * lane;
-        for (uint64_t s = 0; s < nstripes; ++s) acc = xround(acc, ld64u(q + 32 * s));
+        uint64_t s = 0;
+        for (; s + 4 <= nstripes; s += 4) {   // loads of 4 stripes ahead of their rounds
+            const uint64_t v0 = ld(q + 32 * s), v1 = ld(q + 32 * (s + 1));
+            const uint64_t v2 = ld(q + 32 * (s + 2)), v3 = ld(q + 32 * (s + 3));
+            acc = xround(xround(xround(xround(acc, v0), v1), v2), v3);
+        }
+        for (; s < nstripes; ++s) acc = xround(acc, ld(q + 32 * s));
     }
     uint64_t a0 = __shfl_sync(gm, acc, 0, 4), a1 = __shfl_sync(gm, acc, 1, 4);
     uint64_t a2 = __shfl_sync(gm, acc, 2, 4), a3 = __shfl_sync(gm, acc, 3, 4);
@@ -517,6 +540,35 @@ __global__ void k_blob_hash(BlobParams P) {
     if (lane == 0) {
         for (int i = 0; i < 8; ++i) blob[4 + i] = (uint8_t)(h >> (8 * i));
     }
+}
+
+// Device verify (src/mc_archive.c:1072-1111): the chained hash of every
+// listed blob of an archive held in device memory, compared with the hash
+// stored in the blob's header; bad[i] = 1 on a mismatch. 4 lanes per blob.
+__global__ void k_verify_hash(const uint8_t *arc, uint64_t arc_len, const VerifyItem *items, int n, uint32_t *bad) {
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+    const int lane = threadIdx.x & 3;
+    const unsigned gm = 0xFu << ((threadIdx.x & 31) & ~3);
+    if (c >= n) return;   // whole 4-lane groups leave together
+    const VerifyItem it = items[c];
+    const uint8_t *blob = arc + it.co;
+    const FunnelLoad ld{arc + arc_len};
+    const uint16_t fml = (uint16_t)(blob[12] | (blob[13] << 8));
+    const uint8_t *fmap = blob + kBlobHdr, *bm = fmap + fml, *lens = bm + kBitmapBytes;
+    const uint64_t pay = (uint64_t)kBlobHdr + fml + kBitmapBytes + 2ull * it.np;
+    uint64_t h = xxh64_4(fmap, fml, kHashSeed, lane, gm, ld);
+    h ^= xxh64_4(bm, kBitmapBytes, h, lane, gm, ld);
+    h ^= xxh64_4(lens, 2ull * it.np, h, lane, gm, ld);
+    h ^= xxh64_4(blob + pay, it.len - pay, h, lane, gm, ld);
+    if (lane == 0) bad[c] = h != ld64u(blob + 4) ? 1u : 0u;
+}
+
+cudaError_t launch_verify_hash(const uint8_t *d_arc, uint64_t arc_len, const VerifyItem *d_items, int n,
+                               uint32_t *d_bad, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t threads = (int64_t)n * 4;
+    k_verify_hash<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(d_arc, arc_len, d_items, n, d_bad);
+    return cudaGetLastError();
 }
 
 cudaError_t upload_cos_encode(const float cmf[16][16], cudaStream_t s) {

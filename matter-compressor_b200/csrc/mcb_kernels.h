@@ -148,5 +148,13 @@ struct BlobParams {
 cudaError_t launch_blob_layout(const BlobParams &p, cudaStream_t s);   // sizing pass
 cudaError_t launch_blob_fill(const BlobParams &p, cudaStream_t s);     // write pass
 cudaError_t launch_blob_hash(const BlobParams &p, cudaStream_t s);     // xxh64 chain
+// Device verify: blob i at d_arc + co, `len` bytes, np present blocks; its
+// chained xxh64 against the stored one, d_bad[i] = 1 on a mismatch.
+struct VerifyItem {
+    uint64_t co, len;
+    uint32_t np, pad;
+};
+cudaError_t launch_verify_hash(const uint8_t *d_arc, uint64_t arc_len, const VerifyItem *d_items, int n,
+                               uint32_t *d_bad, cudaStream_t s);
 
 }  // namespace mcb

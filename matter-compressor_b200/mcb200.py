@@ -114,6 +114,7 @@ class McLib:
                 "mc_b200_plan_set_config": (i, [vp, vp]),
                 "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
                 "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
+                "mc_b200_verify_archive_dev": (lg, [vp, vp, sz, i]),
                 "mc_b200_append_pyramid": (i, [vp, vp, i, i, i, f, C.POINTER(i)]),
                 "mc_deblock": (None, [vp, i, i, i, f]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
