@@ -300,7 +300,14 @@ def run_regions(args):
     td = tempfile.mkdtemp()
     path = os.path.join(td, "regions.mca")
     a, nch = workloads.build_volume_archive(lib, path, VOLUME_DIMS, lods=8, q=args.q)
+    t0 = time.perf_counter()
     boxes = a.sample_boxes(0, 20260101, 64, 128, 128, 128, 0.5)
+    sample_host_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    boxes_dev = a.sample_boxes_dev(0, 20260101, 64, 128, 128, 128, 0.5)
+    sample_dev_ms = (time.perf_counter() - t0) * 1e3
+    sampling = {"api": "mc_b200_sample_boxes", "boxes": len(boxes), "ms": round(sample_dev_ms, 3),
+                "host_call_ms": round(sample_host_ms, 3), "same_boxes_as_host_call": boxes_dev == boxes}
     crop = 128 ** 3
     stride = crop + 4096                        # strided batch: a 4 KiB gap between crops
     d_out = torch.zeros(stride * len(boxes), dtype=torch.uint8, device="cuda")
@@ -377,6 +384,7 @@ def run_regions(args):
             "plain_host_call": {"api": "mc_archive_read_regions (host output)", "ms": round(host_ms, 3),
                                 "gbs": round(gb / (host_ms / 1e3), 3)},
             "verify": verify,
+            "sampling": sampling,
             "cpu_baseline": cpu}
 
 

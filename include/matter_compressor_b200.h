@@ -187,6 +187,14 @@ int mc_b200_append_chunks(mc_archive *a, mc_codec_ctx *C, int lod, const int *co
  * blobs, like mc_verify_archive (src/matter_compressor.h:370), or -1. */
 long mc_b200_verify_archive_dev(const uint8_t *arc, const uint8_t *d_arc, size_t len, int verbose);
 
+/* mc_archive_sample_boxes with the scoring on the device: the same boxes, in
+ * the same order, from the same seed (src/matter_compressor.h:300). Each
+ * chunk's fraction map is decoded once into a block-fraction grid in device
+ * memory and candidates are scored in batches. Returns the number of boxes
+ * written to out (0 also for a lod outside 0..7 or on a CUDA error). */
+int mc_b200_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count, long dz, long dy, long dx,
+                         float min_frac, mc_box *out);
+
 /* LOD pyramid on the device. mc_b200_decimate_dev: 2x box decimation of a
  * dense DEVICE volume nz x ny x nx into d_dst ((nz+1)/2 x (ny+1)/2 x
  * (nx+1)/2): each output voxel is the rounded mean of its non-zero children,

@@ -29,6 +29,7 @@
 
 #include "mcb_archive.h"
 #include "mcb_host_codec.h"
+#include "mcb_kernels.h"
 #include "mcb_tables.h"
 
 using namespace mcb;
@@ -703,6 +704,73 @@ int mc_archive_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count, lo
                     nb++;
                 }
         if (nb && fsum / nb >= min_frac) { out[got].z0 = z0; out[got].y0 = y0; out[got].x0 = x0; got++; }
+    }
+    return got;
+}
+
+// mc_archive_sample_boxes with the scoring on the device. The fraction map of
+// every chunk that a candidate can touch is decoded once into a block grid
+// (0 where the chunk is absent, all air or has no map, as
+// mc_archive_block_fraction reads it); candidates come from the same
+// xorshift64 stream in the same order, scored a batch at a time; the first
+// `count` accepted ones are the reference's boxes.
+int mc_b200_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count, long dz, long dy, long dx,
+                         float min_frac, mc_box *out) {
+    if (!a || !out || count <= 0 || dz <= 0 || dy <= 0 || dx <= 0 || lod < 0 || lod > 7) return 0;
+    uint32_t unx, uny, unz;
+    memcpy(&unx, a->base + HNX, 4);
+    memcpy(&uny, a->base + HNY, 4);
+    memcpy(&unz, a->base + HNZ, 4);
+    const long NX = (long)unx >> lod, NY = (long)uny >> lod, NZ = (long)unz >> lod;
+    if (NZ < dz || NY < dy || NX < dx) return 0;
+    Lane *L = lane();
+    if (!L) return 0;
+    const long gz = (NZ + 15) >> 4, gy = (NY + 15) >> 4, gx = (NX + 15) >> 4;
+    std::vector<uint8_t> grid((size_t)gz * gy * gx, 0);
+    uint8_t fr[kGrid3];
+    for (long cz = 0; cz * 16 < gz; ++cz)
+        for (long cy = 0; cy * 16 < gy; ++cy)
+            for (long cx = 0; cx * 16 < gx; ++cx) {
+                const uint64_t co = mc_archive_chunk_offset(a, lod, (int)cz, (int)cy, (int)cx);
+                if (co <= kSlotZero) continue;
+                uint16_t fml;
+                memcpy(&fml, a->base + co + 12, 2);
+                if (!fml) continue;
+                host_dec_fracmap(a->base + co + kBlobHdr, fml, fr);
+                for (int b = 0; b < kGrid3; ++b) {
+                    const long bz = cz * 16 + (b >> 8), by = cy * 16 + ((b >> 4) & 15), bx = cx * 16 + (b & 15);
+                    if (bz < gz && by < gy && bx < gx) grid[(size_t)(bz * gy + by) * gx + bx] = fr[b];
+                }
+            }
+    constexpr int B = 4096;   // candidates per scoring launch
+    if (!L->smp_grid.ensure(grid.size()) || !L->smp_cand.ensure(sizeof(long) * 3 * B) || !L->smp_acc.ensure(B) ||
+        !cuda_ok(cudaMemcpyAsync(L->smp_grid.p, grid.data(), grid.size(), cudaMemcpyHostToDevice, L->stream),
+                 "H2D fraction grid"))
+        return 0;
+    uint64_t s = seed ? seed : 0x9E3779B97F4A7C15ull;
+    auto rng = [&s]() { uint64_t x = s; x ^= x << 13; x ^= x >> 7; x ^= x << 17; s = x; return x; };
+    int got = 0;
+    long attempts = 0;
+    const long max_attempts = (long)count * 256;
+    std::vector<long> cand(3 * (size_t)B);
+    std::vector<uint8_t> acc(B);
+    while (got < count && attempts < max_attempts) {
+        const int m = (int)std::min<long>(B, max_attempts - attempts);
+        for (int i = 0; i < m; ++i) {
+            cand[3 * i] = (long)(rng() % (uint64_t)(NZ - dz + 1));
+            cand[3 * i + 1] = (long)(rng() % (uint64_t)(NY - dy + 1));
+            cand[3 * i + 2] = (long)(rng() % (uint64_t)(NX - dx + 1));
+        }
+        attempts += m;
+        if (!cuda_ok(cudaMemcpyAsync(L->smp_cand.p, cand.data(), sizeof(long) * 3 * m, cudaMemcpyHostToDevice,
+                                     L->stream), "H2D candidates") ||
+            !cuda_ok(launch_sample_score(L->smp_grid.as<uint8_t>(), gz, gy, gx, L->smp_cand.as<long>(), m, dz, dy, dx,
+                                         min_frac, L->smp_acc.as<uint8_t>(), L->stream), "sample launch") ||
+            !cuda_ok(cudaMemcpyAsync(acc.data(), L->smp_acc.p, m, cudaMemcpyDeviceToHost, L->stream), "D2H accept") ||
+            !cuda_ok(cudaStreamSynchronize(L->stream), "sync"))
+            return got;
+        for (int i = 0; i < m && got < count; ++i)
+            if (acc[i]) { out[got].z0 = cand[3 * i]; out[got].y0 = cand[3 * i + 1]; out[got].x0 = cand[3 * i + 2]; got++; }
     }
     return got;
 }

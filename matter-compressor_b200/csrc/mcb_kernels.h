@@ -75,6 +75,11 @@ cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s);
 cudaError_t launch_decimate(const uint8_t *d_src, int dz, int dy, int dx, uint8_t *d_dst, cudaStream_t s);
 cudaError_t launch_gather_chunk(const uint8_t *d_src, int nz, int ny, int nx, int cz, int cy, int cx, uint8_t *d_dst,
                                 uint32_t *d_any, cudaStream_t s);
+// Rejection-sampling scores: accept[i] = 1 when candidate box i (z0, y0, x0
+// at d_cand[3i..3i+2], extent dz x dy x dx) has a mean block fraction of at
+// least min_frac over the gz x gy x gx block-fraction grid (nibbles 0..15).
+cudaError_t launch_sample_score(const uint8_t *d_grid, long gz, long gy, long gx, const long *d_cand, int n,
+                                long dz, long dy, long dx, float min_frac, uint8_t *d_accept, cudaStream_t s);
 cudaError_t launch_deblock(uint8_t *d_vol, int count, size_t vstride, int nz, int ny, int nx, int beta, int tc,
                            cudaStream_t s);
 // ---- serving ----

@@ -100,6 +100,7 @@ struct Lane {
     DevBuf b_scratch, b_lens16, b_bitmap, b_fmap, b_fml, b_np, b_len, b_off, b_q, blobs;
     DevBuf pyr_stage, pyr_a, pyr_b, pyr_flag;   // LOD pyramid: chunk staging, level volumes, all-air flags
     DevBuf ver_items, ver_bad;                  // device verify: blob list, mismatch flags
+    DevBuf smp_grid, smp_cand, smp_acc;         // box sampling: block-fraction grid, candidates, accept flags
     HostBuf h_items, h_base, h_stage, h_misc;
     LaunchCfg cfg;
     BlobSlot pipe[2];

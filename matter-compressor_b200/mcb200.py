@@ -115,6 +115,7 @@ class McLib:
                 "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
                 "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
                 "mc_b200_verify_archive_dev": (lg, [vp, vp, sz, i]),
+                "mc_b200_sample_boxes": (i, [vp, i, u64, i, lg, lg, lg, f, vp]),
                 "mc_b200_append_pyramid": (i, [vp, vp, i, i, i, f, C.POINTER(i)]),
                 "mc_deblock": (None, [vp, i, i, i, f]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
@@ -294,6 +295,13 @@ class Archive:
     def sample_boxes(self, lod, seed, count, dz, dy, dx, min_frac):
         arr = (McBox * count)()
         got = self.L.mc_archive_sample_boxes(self.a, lod, seed, count, dz, dy, dx, min_frac, C.cast(arr, C.c_void_p))
+        return [(b.z0, b.y0, b.x0) for b in arr[:got]]
+
+    def sample_boxes_dev(self, lod, seed, count, dz, dy, dx, min_frac):
+        """mc_b200_sample_boxes: the same boxes as sample_boxes, scored on the device."""
+        arr = (McBox * count)()
+        got = self.L.mc_b200_sample_boxes(self.a, lod, seed, count, dz, dy, dx, min_frac, C.cast(arr, C.c_void_p))
+        self.lib.check()
         return [(b.z0, b.y0, b.x0) for b in arr[:got]]
 
     def block_blob(self, co, bz, by, bx):
