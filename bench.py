@@ -311,7 +311,8 @@ def run_regions(args):
     crop = 128 ** 3
     stride = crop + 4096                        # strided batch: a 4 KiB gap between crops
     d_out = torch.zeros(stride * len(boxes), dtype=torch.uint8, device="cuda")
-    s = torch.cuda.current_stream()
+    s = torch.cuda.Stream()   # a real stream: the library treats NULL as its own per-thread stream
+    torch.cuda.set_stream(s)
     for _ in range(args.warmup):
         a.read_regions_dev(0, boxes, 128, 128, 128, d_out.data_ptr(), stride, s.cuda_stream)
     torch.cuda.synchronize()
@@ -407,7 +408,10 @@ def run_deblock(args):
     dec = torch.empty(args.chunks * CHUNK, dtype=torch.uint8, device=dev)
     out = torch.empty_like(dec)
     plan = a.plan_chunks(offs, dec.data_ptr())
-    s = torch.cuda.current_stream()
+    # one non-default stream for every copy, decode and deblock: the library
+    # treats a NULL stream as its own per-thread stream
+    s = torch.cuda.Stream()
+    torch.cuda.set_stream(s)
     plan.launch(s.cuda_stream)
     torch.cuda.synchronize()
     n = args.chunks

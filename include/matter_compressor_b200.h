@@ -148,10 +148,14 @@ int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
 typedef struct mc_b200_plan mc_b200_plan;
 mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *chunk_offs, int n,
                                          mc_u8 *d_out, size_t out_stride);
+/* Replays the plan on `stream` and returns at once. Unlike the other calls,
+ * a NULL stream here is the legacy default stream (the graph launch's own
+ * meaning of NULL), not the library's per-thread stream. */
 int  mc_b200_plan_launch(mc_b200_plan *p, void *stream);
 /* Launch one stage of the plan outside its graph (stage 0: entropy decode,
  * 1: reconstruction; stage 1 consumes stage 0's output), e.g. to time the
- * kernels one by one. */
+ * kernels one by one. Asynchronous on `stream`, NULL = legacy default stream,
+ * as for mc_b200_plan_launch. */
 int  mc_b200_plan_launch_stage(mc_b200_plan *p, int stage, void *stream);
 /* Kernel launches per replay, blocks decoded, and total payload bytes. */
 void mc_b200_plan_info(const mc_b200_plan *p, int *launches, long *blocks, uint64_t *payload_bytes);

@@ -489,11 +489,26 @@ __device__ uint64_t xxh64_4(const uint8_t *p, uint64_t len, uint64_t seed, int l
     if (nstripes) {
         acc = lane == 0 ? seed + XP1 + XP2 : lane == 1 ? seed + XP2 : lane == 2 ? seed : seed - XP1;
         const uint8_t *q = p + 8 * lane;
+        // Batches of 8 stripes, double-buffered in registers: the loads of the
+        // next batch are in flight while this batch's rounds (a serial chain)
+        // run, so a lane waits on memory once per stream, not once per batch.
+        constexpr int K = 8;
         uint64_t s = 0;
-        for (; s + 4 <= nstripes; s += 4) {   // loads of 4 stripes ahead of their rounds
-            const uint64_t v0 = ld(q + 32 * s), v1 = ld(q + 32 * (s + 1));
-            const uint64_t v2 = ld(q + 32 * (s + 2)), v3 = ld(q + 32 * (s + 3));
-            acc = xround(xround(xround(xround(acc, v0), v1), v2), v3);
+        if (nstripes >= K) {
+            uint64_t cur[K], nxt[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) cur[j] = ld(q + 32 * j);
+            for (; s + 2 * K <= nstripes; s += K) {
+#pragma unroll
+                for (int j = 0; j < K; ++j) nxt[j] = ld(q + 32 * (s + K + j));
+#pragma unroll
+                for (int j = 0; j < K; ++j) acc = xround(acc, cur[j]);
+#pragma unroll
+                for (int j = 0; j < K; ++j) cur[j] = nxt[j];
+            }
+#pragma unroll
+            for (int j = 0; j < K; ++j) acc = xround(acc, cur[j]);
+            s += K;
         }
         for (; s < nstripes; ++s) acc = xround(acc, ld(q + 32 * s));
     }
