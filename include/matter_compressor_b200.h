@@ -109,6 +109,24 @@ uint64_t mc_xxh64(const void *data, size_t len, uint64_t seed);            /* sr
  * device). A read past the volume's end, undefined in the reference, reads 0. */
 void mc_deblock(mc_u8 *vol, int nz, int ny, int nx, float quality);      /* src/matter_compressor.h:106 */
 
+/* ---- read-only readers (blocks decoded on the GPU) ---- */
+typedef struct mc_reader mc_reader;
+typedef int (*mc_read_fn)(void *ud, uint64_t off, uint32_t len, uint8_t *dst);        /* :329 */
+mc_reader *mc_open(const uint8_t *arc, size_t len);                                     /* :316 */
+void       mc_close(mc_reader *r);                                                      /* :317 */
+void       mc_reader_set_quality(mc_reader *r, float q);                                /* :318 */
+uint64_t   mc_chunk_offset(mc_reader *r, int lod, int cz, int cy, int cx);              /* :319 */
+uint64_t   mc_chunk_offset_chk(mc_reader *r, int lod, int cz, int cy, int cx, int *err); /* :323 */
+void       mc_decode_block(mc_reader *r, uint64_t chunk_off, int bz, int by, int bx, mc_u8 *dst); /* :324 */
+mc_reader *mc_open_streaming(mc_read_fn read, void *ud, uint64_t total_len);           /* :334 */
+void       mc_reader_set_partial_fetch(mc_reader *r, int on);                           /* :341 */
+uint64_t   mc_reader_chunk_blob_len(mc_reader *r, uint64_t chunk_off);                  /* :346 */
+int        mc_reader_read_blob(mc_reader *r, uint64_t chunk_off, size_t len, uint8_t *dst); /* :352 */
+int        mc_reader_priors(mc_reader *r, const uint16_t **plo, const uint16_t **phi);  /* :356 */
+void       mc_reader_dims(mc_reader *r, int *nx, int *ny, int *nz);                     /* :359 */
+float      mc_reader_quality(mc_reader *r);                                             /* :360 */
+int        mc_reader_nlods(mc_reader *r);                                               /* :361 */
+
 /* ====================================================== part 2: additions */
 
 /* Runtime. mc_b200_init returns 0 when an sm_100 device is usable, -1 (with
@@ -198,6 +216,17 @@ long mc_b200_verify_archive_dev(const uint8_t *arc, const uint8_t *d_arc, size_t
  * written to out (0 also for a lod outside 0..7 or on a CUDA error). */
 int mc_b200_sample_boxes(mc_archive *a, int lod, uint64_t seed, int count, long dz, long dy, long dx,
                          float min_frac, mc_box *out);
+
+/* Reader batch decode: n blocks (bz, by, bx) = coords[3i..3i+2] of the chunk
+ * at chunk_off into DEVICE memory, block i at d_out + 4096*i (16^3, z,y,x),
+ * decoded on the GPU in one batch, the same voxels mc_decode_block gives.
+ * Flat and full-fetch readers copy the payloads from the chunk blob; a
+ * partial-fetch streaming reader reads only the asked-for payloads, one range
+ * read per run of adjacent ones. Absent blocks, a missing chunk and unreadable
+ * bytes decode to zeros. Returns 0 (after the decode ends), -1 on bad
+ * arguments or a CUDA error. */
+int mc_b200_reader_decode_blocks(mc_reader *r, uint64_t chunk_off, const int *coords, int n, mc_u8 *d_out,
+                                 void *stream);
 
 /* LOD pyramid on the device. mc_b200_decimate_dev: 2x box decimation of a
  * dense DEVICE volume nz x ny x nx into d_dst ((nz+1)/2 x (ny+1)/2 x

@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-ftz=false", "-prec-div=true", "-prec-sqrt=true",
           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math,-Wall", "-I", CSRC]
 SOURCES = ["mcb_decode.cu", "mcb_encode.cu", "mcb_tables.cpp", "mcb_runtime.cpp", "mcb_host_codec.cpp",
-           "mcb_archive.cpp", "mcb_api.cpp", "mcb_noalloc.cu", "mcb_gather.cu", "mcb_server.cpp", "mcb_deblock.cu", "mcb_lod.cu", "mcb_sample.cu"]
+           "mcb_archive.cpp", "mcb_api.cpp", "mcb_noalloc.cu", "mcb_gather.cu", "mcb_server.cpp", "mcb_deblock.cu", "mcb_lod.cu", "mcb_sample.cu", "mcb_reader.cpp"]
 
 
 def _stale(obj, deps):

@@ -462,20 +462,9 @@ __device__ __forceinline__ uint32_t ld32u(const uint8_t *p) {
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
 
-// Stripe loaders: bytes one at a time (any address), or two aligned 64-bit
-// loads joined by a funnel shift when both words lie below `limit`.
+// Stripe loader: bytes one at a time (any address).
 struct ByteLoad {
     __device__ uint64_t operator()(const uint8_t *p) const { return ld64u(p); }
-};
-struct FunnelLoad {
-    const uint8_t *limit;
-    __device__ uint64_t operator()(const uint8_t *p) const {
-        const uint32_t a = (uint32_t)((uintptr_t)p & 7);
-        const uint64_t *w = reinterpret_cast<const uint64_t *>(p - a);
-        if (reinterpret_cast<const uint8_t *>(w + 2) > limit) return ld64u(p);
-        const uint64_t lo = __ldg(w), hi = __ldg(w + 1);
-        return a ? (lo >> (8 * a)) | (hi << (64 - 8 * a)) : lo;
-    }
 };
 
 // XXH64 computed by 4 cooperating lanes (lanes 0..3 of a warp): lane i owns
@@ -559,30 +548,124 @@ __global__ void k_blob_hash(BlobParams P) {
 
 // Device verify (src/mc_archive.c:1072-1111): the chained hash of every
 // listed blob of an archive held in device memory, compared with the hash
-// stored in the blob's header; bad[i] = 1 on a mismatch. 4 lanes per blob.
-__global__ void k_verify_hash(const uint8_t *arc, uint64_t arc_len, const VerifyItem *items, int n, uint32_t *bad) {
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
-    const int lane = threadIdx.x & 3;
-    const unsigned gm = 0xFu << ((threadIdx.x & 31) & ~3);
-    if (c >= n) return;   // whole 4-lane groups leave together
+// stored in the blob's header; bad[i] = 1 on a mismatch.
+//
+// One warp per blob. XXH64 keeps 4 serial accumulators, so 4 lanes hash; the
+// whole warp first brings each 4 KiB tile of the blob into shared memory with
+// coalesced 16-byte loads (many in flight at once), and the hashing lanes then
+// read their stripes from shared memory: the serial round chain no longer
+// waits on memory for every stripe.
+namespace {
+constexpr int kVerifyWarps = 4;
+constexpr int kTileStripes = 128;
+constexpr int kTileBytes = kTileStripes * 32;
+constexpr int kTileBuf = kTileBytes + 64;   // a window plus its misaligned head and tail
+
+// Bytes [start, start + n) of the archive into tile (n <= kTileBytes + 32),
+// from the 16-byte boundary at or below start; bytes outside [base, limit)
+// read 0. Returns that boundary. Every lane of the warp calls it.
+__device__ const uint8_t *load_window(const uint8_t *base, const uint8_t *limit, const uint8_t *start, uint32_t n,
+                                      uint8_t *tile) {
+    const int lane = threadIdx.x & 31;
+    const uint8_t *wb = reinterpret_cast<const uint8_t *>((uintptr_t)start & ~(uintptr_t)15);
+    const uint32_t nvec = (uint32_t)((start + n - wb + 15) / 16);
+    for (uint32_t i = lane; i < nvec; i += 32) {
+        const uint8_t *q = wb + 16 * i;
+        uint4 v;
+        if (q >= base && q + 16 <= limit) {
+            v = __ldg(reinterpret_cast<const uint4 *>(q));
+        } else {
+            uint8_t b[16];
+            for (int k = 0; k < 16; ++k) b[k] = (q + k >= base && q + k < limit) ? q[k] : 0;
+            memcpy(&v, b, 16);
+        }
+        reinterpret_cast<uint4 *>(tile)[i] = v;
+    }
+    __syncwarp();
+    return wb;
+}
+
+// 8 little-endian bytes at tile offset o (any alignment)
+__device__ __forceinline__ uint64_t tile64(const uint8_t *tile, uint32_t o) {
+    const uint32_t a = o & 7;
+    const uint64_t lo = *reinterpret_cast<const uint64_t *>(tile + (o - a));
+    if (!a) return lo;
+    const uint64_t hi = *reinterpret_cast<const uint64_t *>(tile + (o - a) + 8);
+    return (lo >> (8 * a)) | (hi << (64 - 8 * a));
+}
+
+// XXH64 of [p, p + len) by a whole warp through tile; the hash in every lane.
+__device__ uint64_t xxh64_warp(const uint8_t *base, const uint8_t *limit, const uint8_t *p, uint64_t len,
+                               uint64_t seed, uint8_t *tile) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nstripes = len >= 32 ? len / 32 : 0;
+    uint64_t acc = lane == 0 ? seed + XP1 + XP2 : lane == 1 ? seed + XP2 : lane == 2 ? seed : seed - XP1;
+    for (uint64_t s0 = 0; s0 < nstripes; s0 += kTileStripes) {
+        const uint32_t n = (uint32_t)min((uint64_t)kTileStripes, nstripes - s0);
+        const uint8_t *start = p + 32 * s0;
+        const uint8_t *wb = load_window(base, limit, start, 32 * n, tile);
+        if (lane < 4) {
+            const uint32_t o0 = (uint32_t)(start - wb) + 8 * lane;
+#pragma unroll 8
+            for (uint32_t s = 0; s < n; ++s) acc = xround(acc, tile64(tile, o0 + 32 * s));
+        }
+        __syncwarp();
+    }
+    const uint64_t a0 = __shfl_sync(0xFFFFFFFFu, acc, 0), a1 = __shfl_sync(0xFFFFFFFFu, acc, 1);
+    const uint64_t a2 = __shfl_sync(0xFFFFFFFFu, acc, 2), a3 = __shfl_sync(0xFFFFFFFFu, acc, 3);
+    uint64_t h;
+    if (nstripes) {
+        h = rotl64(a0, 1) + rotl64(a1, 7) + rotl64(a2, 12) + rotl64(a3, 18);
+        h = (h ^ xround(0, a0)) * XP1 + XP4;
+        h = (h ^ xround(0, a1)) * XP1 + XP4;
+        h = (h ^ xround(0, a2)) * XP1 + XP4;
+        h = (h ^ xround(0, a3)) * XP1 + XP4;
+    } else {
+        h = seed + XP5;
+    }
+    h += len;
+    // the tail (< 32 bytes) by every lane alike, from one more window
+    const uint8_t *t = p + nstripes * 32;
+    const uint32_t rem = (uint32_t)(len - nstripes * 32);
+    const uint8_t *wb = load_window(base, limit, t, rem, tile);
+    uint32_t o = (uint32_t)(t - wb), end = o + rem;
+    for (; end - o >= 8; o += 8) h = rotl64(h ^ xround(0, tile64(tile, o)), 27) * XP1 + XP4;
+    if (end - o >= 4) {
+        const uint64_t w = tile64(tile, o) & 0xFFFFFFFFull;
+        h = rotl64(h ^ (w * XP1), 23) * XP2 + XP3;
+        o += 4;
+    }
+    for (; o < end; ++o) h = rotl64(h ^ ((uint64_t)tile[o] * XP5), 11) * XP1;
+    h ^= h >> 33; h *= XP2; h ^= h >> 29; h *= XP3; h ^= h >> 32;
+    __syncwarp();   // the tile is reused by the next call
+    return h;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kVerifyWarps * 32) k_verify_hash(const uint8_t *arc, uint64_t arc_len,
+                                                                   const VerifyItem *items, int n, uint32_t *bad) {
+    __shared__ __align__(16) uint8_t s_tile[kVerifyWarps][kTileBuf];
+    const int w = threadIdx.x >> 5;
+    const int c = blockIdx.x * kVerifyWarps + w;
+    if (c >= n) return;   // whole warps leave together
+    uint8_t *tile = s_tile[w];
     const VerifyItem it = items[c];
-    const uint8_t *blob = arc + it.co;
-    const FunnelLoad ld{arc + arc_len};
+    const uint8_t *blob = arc + it.co, *limit = arc + arc_len;
     const uint16_t fml = (uint16_t)(blob[12] | (blob[13] << 8));
     const uint8_t *fmap = blob + kBlobHdr, *bm = fmap + fml, *lens = bm + kBitmapBytes;
     const uint64_t pay = (uint64_t)kBlobHdr + fml + kBitmapBytes + 2ull * it.np;
-    uint64_t h = xxh64_4(fmap, fml, kHashSeed, lane, gm, ld);
-    h ^= xxh64_4(bm, kBitmapBytes, h, lane, gm, ld);
-    h ^= xxh64_4(lens, 2ull * it.np, h, lane, gm, ld);
-    h ^= xxh64_4(blob + pay, it.len - pay, h, lane, gm, ld);
-    if (lane == 0) bad[c] = h != ld64u(blob + 4) ? 1u : 0u;
+    uint64_t h = xxh64_warp(arc, limit, fmap, fml, kHashSeed, tile);
+    h ^= xxh64_warp(arc, limit, bm, kBitmapBytes, h, tile);
+    h ^= xxh64_warp(arc, limit, lens, 2ull * it.np, h, tile);
+    h ^= xxh64_warp(arc, limit, blob + pay, it.len - pay, h, tile);
+    if ((threadIdx.x & 31) == 0) bad[c] = h != ld64u(blob + 4) ? 1u : 0u;
 }
 
 cudaError_t launch_verify_hash(const uint8_t *d_arc, uint64_t arc_len, const VerifyItem *d_items, int n,
                                uint32_t *d_bad, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    const int64_t threads = (int64_t)n * 4;
-    k_verify_hash<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(d_arc, arc_len, d_items, n, d_bad);
+    k_verify_hash<<<(unsigned)((n + kVerifyWarps - 1) / kVerifyWarps), kVerifyWarps * 32, 0, s>>>(d_arc, arc_len,
+                                                                                                d_items, n, d_bad);
     return cudaGetLastError();
 }
 

@@ -116,6 +116,20 @@ class McLib:
                 "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
                 "mc_b200_verify_archive_dev": (lg, [vp, vp, sz, i]),
                 "mc_b200_sample_boxes": (i, [vp, i, u64, i, lg, lg, lg, f, vp]),
+                "mc_open": (vp, [vp, sz]),
+                "mc_open_streaming": (vp, [vp, vp, u64]),
+                "mc_close": (None, [vp]),
+                "mc_reader_set_quality": (None, [vp, f]),
+                "mc_reader_set_partial_fetch": (None, [vp, i]),
+                "mc_chunk_offset": (u64, [vp, i, i, i, i]),
+                "mc_chunk_offset_chk": (u64, [vp, i, i, i, i, C.POINTER(i)]),
+                "mc_decode_block": (None, [vp, u64, i, i, i, vp]),
+                "mc_reader_chunk_blob_len": (u64, [vp, u64]),
+                "mc_reader_read_blob": (i, [vp, u64, sz, vp]),
+                "mc_reader_dims": (None, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
+                "mc_reader_quality": (f, [vp]),
+                "mc_reader_nlods": (i, [vp]),
+                "mc_b200_reader_decode_blocks": (i, [vp, u64, vp, i, vp, vp]),
                 "mc_b200_append_pyramid": (i, [vp, vp, i, i, i, f, C.POINTER(i)]),
                 "mc_deblock": (None, [vp, i, i, i, f]),
                 "mc_b200_append_chunks": (i, [vp, vp, i, vp, i, vp, i, f]),
@@ -478,3 +492,103 @@ def decode_chunk_blobs(lib, blobs, out=None):
     if rc:
         raise RuntimeError("mc_b200_decode_chunk_blobs failed")
     return out
+
+
+READ_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p)
+_READER_SIGS = {
+    "mc_open": (C.c_void_p, [C.c_void_p, C.c_size_t]),
+    "mc_open_streaming": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "mc_close": (None, [C.c_void_p]),
+    "mc_reader_set_quality": (None, [C.c_void_p, C.c_float]),
+    "mc_reader_set_partial_fetch": (None, [C.c_void_p, C.c_int]),
+    "mc_chunk_offset": (C.c_uint64, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "mc_chunk_offset_chk": (C.c_uint64, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "mc_decode_block": (None, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "mc_reader_chunk_blob_len": (C.c_uint64, [C.c_void_p, C.c_uint64]),
+    "mc_reader_read_blob": (C.c_int, [C.c_void_p, C.c_uint64, C.c_size_t, C.c_void_p]),
+    "mc_reader_dims": (None, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mc_reader_quality": (C.c_float, [C.c_void_p]),
+    "mc_reader_nlods": (C.c_int, [C.c_void_p]),
+}
+
+
+class Reader:
+    """A read-only reader (mc_open / mc_open_streaming) of either library:
+    over archive bytes in memory, or over a file through a byte-range
+    callback that counts the bytes and calls it serves."""
+
+    def __init__(self, lib, data=None, path=None, partial=False):
+        L = self.L = lib.L
+        self.lib = lib
+        for name, (res, args) in _READER_SIGS.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        self.bytes = self.calls = 0
+        if data is not None:
+            self.data = np.ascontiguousarray(np.frombuffer(data, np.uint8))
+            self.r = L.mc_open(self.data.ctypes.data, self.data.size)
+        else:
+            self.f = open(path, "rb")
+            size = os.path.getsize(path)
+
+            def read(ud, off, n, dst):
+                if off + n > size:
+                    return -1
+                self.f.seek(off)
+                b = self.f.read(n)
+                C.memmove(dst, b, n)
+                self.bytes += n
+                self.calls += 1
+                return 0
+            self._cb = READ_FN(read)
+            self.r = L.mc_open_streaming(C.cast(self._cb, C.c_void_p), None, size)
+            if partial:
+                L.mc_reader_set_partial_fetch(self.r, 1)
+        if not self.r:
+            raise RuntimeError("reader open failed")
+
+    def close(self):
+        if self.r:
+            self.L.mc_close(self.r)
+            self.r = None
+        if hasattr(self, "f"):
+            self.f.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def chunk_offset(self, lod, cz, cy, cx):
+        return self.L.mc_chunk_offset(self.r, lod, cz, cy, cx)
+
+    def chunk_offset_chk(self, lod, cz, cy, cx):
+        err = C.c_int()
+        co = self.L.mc_chunk_offset_chk(self.r, lod, cz, cy, cx, C.byref(err))
+        return co, err.value
+
+    def decode_block(self, co, bz, by, bx):
+        out = np.zeros(4096, np.uint8)
+        self.L.mc_decode_block(self.r, co, bz, by, bx, out.ctypes.data)
+        return out
+
+    def blob(self, co):
+        n = self.L.mc_reader_chunk_blob_len(self.r, co)
+        out = np.zeros(n, np.uint8)
+        if n and self.L.mc_reader_read_blob(self.r, co, n, out.ctypes.data) != 0:
+            return None
+        return out.tobytes()
+
+    def info(self):
+        x, y, z = C.c_int(), C.c_int(), C.c_int()
+        self.L.mc_reader_dims(self.r, C.byref(x), C.byref(y), C.byref(z))
+        return (x.value, y.value, z.value), self.L.mc_reader_quality(self.r), self.L.mc_reader_nlods(self.r)
+
+    def decode_blocks_dev(self, co, coords, d_out, stream=None):
+        """mc_b200_reader_decode_blocks (this library only)."""
+        cc = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1))
+        rc = self.L.mc_b200_reader_decode_blocks(self.r, co, cc.ctypes.data, len(coords), C.c_void_p(d_out),
+                                                 C.c_void_p(stream) if stream else None)
+        self.lib.check()
+        return rc

@@ -98,3 +98,44 @@ def test_sampler_and_fractions_match_reference(tmp_path, ref, golden_chunks):
                     for bx in (0, 9, 33)]
         res.append((boxes, fr, pres))
     assert res[0] == res[1]
+
+
+def test_readers_host_side_match_reference(tmp_path, ref, golden_chunks):
+    """mc_open / mc_open_streaming (full and partial fetch): chunk resolution
+    (absent, present, out-of-range LOD, failed reads), blob length and bytes,
+    dims, quality and LOD count == the reference's readers on the same file."""
+    from mcb200 import Reader
+    path = str(tmp_path / "r.mca")
+    data, _ = replay(ref, path, golden_chunks)
+    mine_lib = product_host()
+    coords = [(lod, cz, cy, cx) for lod in range(-1, 9) for cz in range(4) for cy in range(2) for cx in range(4)]
+    for kind in ("flat", "full", "partial"):
+        def mk(lib):
+            if kind == "flat":
+                return Reader(lib, data=data)
+            return Reader(lib, path=path, partial=kind == "partial")
+        with mk(mine_lib) as m, mk(ref) as r:
+            assert m.info() == r.info()
+            for c in coords:
+                assert m.chunk_offset_chk(*c) == r.chunk_offset_chk(*c), (kind, c)
+                co = r.chunk_offset(*c)
+                if co > 1:
+                    assert m.blob(co) == r.blob(co) == data[co:co + shapes.blob_len(data, co)]
+    # a byte source that fails after the header reports err=1, not an absent chunk
+    import ctypes as C
+    from mcb200 import READ_FN
+    hdr = data[:256]
+
+    def read(ud, off, n, dst):
+        if off + n > len(hdr):
+            return -1
+        C.memmove(dst, hdr[off:off + n], n)
+        return 0
+    cb = READ_FN(read)
+    for lib in (mine_lib, ref):
+        Reader(lib, data=data).close()   # binds the reader signatures
+        r = lib.L.mc_open_streaming(C.cast(cb, C.c_void_p), None, len(data))
+        err = C.c_int()
+        assert lib.L.mc_chunk_offset_chk(r, 0, 0, 0, 0, C.byref(err)) == 0 and err.value == 1
+        assert lib.L.mc_chunk_offset_chk(r, 7, 0, 0, 0, C.byref(err)) == 0 and err.value == 0   # no root
+        lib.L.mc_close(r)
