@@ -16,7 +16,9 @@
 //
 // Memory: the x pass touches every 32-byte sector of the volume (faces every
 // 16 bytes), the y and z passes a quarter of the rows and planes, so one call
-// moves about 2.75x the volume's bytes.
+// moves about 2.75x the volume's bytes. Where rows are 16-byte aligned the y
+// and z passes take 16 faces per thread as 16-byte row vectors (four
+// independent loads in flight per thread instead of four single bytes).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -80,6 +82,53 @@ __global__ void __launch_bounds__(256) k_deblock_z(DbParams P) {
     }
 }
 
+// The same filter on 16 faces side by side in x: rows p1, p0, q0, q1 as
+// 16-byte vectors; p0 and q0 come back. Used when rows are 16-byte aligned.
+__device__ __forceinline__ void db_face16(uint8_t *v, size_t total, size_t i, size_t step, int beta, int tc) {
+    const uint4 P1 = *reinterpret_cast<const uint4 *>(v + i - 2 * step);
+    uint4 P0 = *reinterpret_cast<const uint4 *>(v + i - step);
+    uint4 Q0 = *reinterpret_cast<const uint4 *>(v + i);
+    const uint4 Q1 = i + step < total ? *reinterpret_cast<const uint4 *>(v + i + step) : make_uint4(0, 0, 0, 0);
+    const uint8_t *p1 = reinterpret_cast<const uint8_t *>(&P1), *q1 = reinterpret_cast<const uint8_t *>(&Q1);
+    uint8_t *p0 = reinterpret_cast<uint8_t *>(&P0), *q0 = reinterpret_cast<uint8_t *>(&Q0);
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+        const int a = p0[b], c = q0[b];
+        if (a == 0 || c == 0) continue;
+        const int d = c - a;
+        if (abs(d) >= beta) continue;
+        const int pn = p1[b] ? p1[b] : a, qn = q1[b] ? q1[b] : c;
+        int delta = (4 * d + (pn - qn) + 4) >> 3;
+        delta = delta > tc ? tc : delta;
+        delta = delta < -tc ? -tc : delta;
+        p0[b] = (uint8_t)min(max(a + delta, 1), 255);
+        q0[b] = (uint8_t)min(max(c - delta, 1), 255);
+    }
+    *reinterpret_cast<uint4 *>(v + i - step) = P0;
+    *reinterpret_cast<uint4 *>(v + i) = Q0;
+}
+
+// y faces, 16 x at a time: work = nz x nf x (nx/16).
+__global__ void __launch_bounds__(256) k_deblock_y16(DbParams P) {
+    uint8_t *v = P.vol + (size_t)blockIdx.y * P.vstride;
+    const uint32_t nxs = P.nx >> 4;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < P.work; g += gridDim.x * blockDim.x) {
+        const uint32_t t = g / nxs, xs = g - t * nxs;
+        const uint32_t z = t / P.nf, k = t - z * P.nf;
+        db_face16(v, P.total, (size_t)z * P.sz + (size_t)(16u * (k + 1u)) * P.nx + 16u * xs, P.nx, P.beta, P.tc);
+    }
+}
+
+// z faces, 16 x at a time: work = nf x (ny*nx/16).
+__global__ void __launch_bounds__(256) k_deblock_z16(DbParams P) {
+    uint8_t *v = P.vol + (size_t)blockIdx.y * P.vstride;
+    const uint32_t s16 = P.sz >> 4;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < P.work; g += gridDim.x * blockDim.x) {
+        const uint32_t k = g / s16, r = g - k * s16;
+        db_face16(v, P.total, (size_t)(16u * (k + 1u)) * P.sz + 16u * r, P.sz, P.beta, P.tc);
+    }
+}
+
 static int db_sms() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -118,12 +167,20 @@ cudaError_t launch_deblock(uint8_t *d_vol, int count, size_t vstride, int nz, in
     P.nf = faces(P.nx);
     P.work = (uint32_t)(rows * P.nf);
     if (P.work) k_deblock_x<<<grid(P.work), 256, 0, s>>>(P);
+    // rows of 16-byte vectors when every row of every volume starts on a 16-byte boundary
+    const bool vec = nx % 16 == 0 && ((uintptr_t)d_vol & 15) == 0 && (count == 1 || vstride % 16 == 0);
     P.nf = faces(P.ny);
-    P.work = P.nz * P.nf * P.nx;
-    if (P.work) k_deblock_y<<<grid(P.work), 256, 0, s>>>(P);
+    P.work = P.nz * P.nf * (vec ? P.nx / 16 : P.nx);
+    if (P.work) {
+        if (vec) k_deblock_y16<<<grid(P.work), 256, 0, s>>>(P);
+        else k_deblock_y<<<grid(P.work), 256, 0, s>>>(P);
+    }
     P.nf = faces(P.nz);
-    P.work = P.nf * P.sz;
-    if (P.work) k_deblock_z<<<grid(P.work), 256, 0, s>>>(P);
+    P.work = P.nf * (vec ? P.sz / 16 : P.sz);
+    if (P.work) {
+        if (vec) k_deblock_z16<<<grid(P.work), 256, 0, s>>>(P);
+        else k_deblock_z<<<grid(P.work), 256, 0, s>>>(P);
+    }
     return cudaGetLastError();
 }
 
