@@ -38,7 +38,7 @@ __constant__ float c_cos[16][16];
 // block. The block header (flags, dc, EOB) is decoded when a lane starts its
 // block.
 enum : uint32_t {
-    F_SIG = 0,   // significance of scan position p: context sigb + min(cnt, 3)
+    F_SIG = 0,   // significance of scan position p: context sigb + min(popcount(last 16 flags), 3)
     F_MAG,       // unary magnitude rung k: context 56 + k
     F_SIGN,      // sign (bypass) of the coefficient at p, magnitude m
     F_EGP,       // Exp-Golomb prefix (bypass): k counts 12 + the one-bits so far
@@ -66,7 +66,7 @@ struct LaneState {
     uint32_t len, off0;        // payload length, payload start - abase
     uint32_t w, nxt, sel, jn;  // window word, next word, byte selector, index of the next word
     uint32_t code, range;
-    uint32_t st, p, eob, cnt, hist, sigb, band, bend, stop, k, m;
+    uint32_t st, p, eob, hist, sigb, band, bend, stop, k, m;   // hist: significance flags, newest in bit 0
     uint32_t cc, pc;           // context slot of the next bin and its probability (coefficient loop)
     uint32_t hdr;              // flag0, flag1, dc bits 7..0 (10 bits, first bin highest)
     uint32_t rem, acc, ret;
@@ -156,7 +156,8 @@ __device__ __forceinline__ bool put_entry(LaneState &L, const EntParams &P, uint
 // Context slot of the bin the lane's state asks for next and its current
 // value; bypass states use the scratch slot.
 __device__ __forceinline__ void load_ctx(LaneState &L, const uint32_t *ctx) {
-    L.cc = L.st == F_SIG ? L.sigb + min(L.cnt, 3u) : (L.st == F_MAG ? (uint32_t)kCtxMag + L.k : kSignSlot);
+    L.cc = L.st == F_SIG ? L.sigb + min((uint32_t)__popc(L.hist & 0xFFFFu), 3u)
+                         : (L.st == F_MAG ? (uint32_t)kCtxMag + L.k : kSignSlot);
     L.pc = ctx[L.cc * 32];
 }
 
@@ -172,7 +173,6 @@ __device__ __forceinline__ void position_event(LaneState &L, const uint32_t *ctx
     if (L.p + 1 >= L.eob) {
         if (L.p + 1 == L.eob) {
             L.hist = (L.hist << 1) | 1u;
-            L.cnt = L.cnt + 1u - ((L.hist >> 16) & 1u);
             L.st = F_MAG;
             L.k = 0;
         } else {
@@ -200,7 +200,7 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
     L.nent = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
     L.hdr = 0;
     L.rem = 0; L.acc = 0; L.ret = R_MAG;
-    L.p = 0; L.eob = 0; L.hist = 0; L.cnt = 0; L.k = 0; L.m = 0;
+    L.p = 0; L.eob = 0; L.hist = 0; L.k = 0; L.m = 0;
     L.band = 0; L.sigb = kCtxSig; L.bend = s_bend[0]; L.stop = 0;
     if (L.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
     const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[it.qslot].ctx);
@@ -339,9 +339,10 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     const bool is_sig = st == F_SIG, is_mag = st == F_MAG, is_sign = st == F_SIGN, is_egp = st == F_EGP;
     const bool is_byp = is_sign | is_egp;
     // candidate contexts of the next bin: c0 if this bin is 0, c1 if it is 1
-    const uint32_t out = (L.hist >> 15) & 1u;
     const uint32_t k1 = L.k + 1u;
-    const uint32_t sig_next = L.sigb + min(L.cnt - (is_sig ? out : 0u), 3u);
+    // significant flags among the last 16 positions once this bin (if a
+    // significance bin) has come out 0: the window then drops its oldest flag
+    const uint32_t sig_next = L.sigb + min((uint32_t)__popc(L.hist & (is_sig ? 0x7FFFu : 0xFFFFu)), 3u);
     const uint32_t c0 = (is_sig | is_sign) ? sig_next : kSignSlot;
     const uint32_t c1 = is_sig ? (uint32_t)kCtxMag
                                : (is_mag ? (k1 < 12u ? (uint32_t)kCtxMag + k1 : kSignSlot) : c0);
@@ -367,9 +368,8 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     L.pc = (INNER || live) ? ((ncc == L.cc && !is_byp) ? np0 : nq) : L.pc;
     L.cc = (INNER || live) ? ncc : L.cc;
 
-    // significance history (the flag leaving the 16-position window drops out of cnt)
+    // significance history
     L.hist = is_sig ? (L.hist << 1) | b : L.hist;
-    L.cnt = is_sig ? L.cnt + b - out : L.cnt;
     const uint32_t m = L.m;
     L.m = is_mag ? k1 : m;
     const bool esc = is_mag & bit & (L.k == 11);            // 12th rung set: Exp-Golomb tail
@@ -626,8 +626,27 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         if (tid < 3) s_ext[tid] = 0;
         if (tid == 3) s_l1 = 0.0f;
         __syncthreads();
+        // A thread's first kKeep entries stay in registers for the
+        // dequantisation, as raster index | level << 16: blocks of up to
+        // 128 * kKeep entries read their entry list and scan table once.
+        constexpr int kKeep = 4;
+        uint32_t keep[kKeep];
         int mz = 0, my = 0, mx = 0;
-        for (int j = tid; j < nnz; j += 128) {
+#pragma unroll
+        for (int k = 0; k < kKeep; ++k) {
+            const int j = tid + 128 * k;
+            uint32_t v = 0;
+            if (j < nnz) {
+                const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
+                const uint32_t idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFFu;
+                v = idx | (e & 0xFFFF0000u);
+                mz = max(mz, (int)((idx >> 8) & 15));
+                my = max(my, (int)((idx >> 4) & 15));
+                mx = max(mx, (int)(idx & 15));
+            }
+            keep[k] = v;
+        }
+        for (int j = tid + 128 * kKeep; j < nnz; j += 128) {
             const uint32_t e = __ldg(P.scan + (entry_at<CG>(P, base, cap, h.ovf, j) & 0xFFFu)) & 0xFFFu;
             mz = max(mz, (int)((e >> 8) & 15));
             my = max(my, (int)((e >> 4) & 15));
@@ -649,18 +668,24 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         __syncthreads();
         // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
         float l1 = 0.0f;
-        for (int j = tid; j < nnz; j += 128) {
-            const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
-            const int idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFF;
-            const int lv = (int16_t)(e >> 16);
-            if (!lv) continue;
+        auto dequant = [&](uint32_t v) {   // v: raster index | level << 16
+            const int idx = (int)(v & 0xFFFu);
+            const int lv = (int16_t)(v >> 16);
+            if (!lv) return;
             const int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;
-            if (cz >= E || cy >= Y || cx >= X) continue;
+            if (cz >= E || cy >= Y || cx >= X) return;
             const int f = cz + cy + cx;
             const float a = (float)(lv < 0 ? -lv : lv);
             const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
             sB[(cz * Y + cy) * X + cx] = lv < 0 ? -r : r;
             l1 = fadd(l1, r);
+        };
+#pragma unroll
+        for (int k = 0; k < kKeep; ++k)
+            if (tid + 128 * k < nnz) dequant(keep[k]);
+        for (int j = tid + 128 * kKeep; j < nnz; j += 128) {
+            const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
+            dequant((__ldg(P.scan + (e & 0xFFFu)) & 0xFFFu) | (e & 0xFFFF0000u));
         }
         // the L1 norm only bounds the voxels: any summation order will do
         for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xFFFFFFFFu, l1, o);
