@@ -597,11 +597,22 @@ constexpr int kStageBytes = 16 * kStageZ;
 // Reconstruct one block into a stage (z slices of kStageZ bytes). Thread t owns the
 // output pair (m, m+1) = 2*(t&3) of every line it touches; its cosine weights
 // come from the shared table W.
+// next: the item this CTA reconstructs after this one (-1: none). While this
+// block's transform runs, the start of the next block's entry list is
+// prefetched into L2, so that its loads do not wait on DRAM.
 template <bool CG>
 __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, float *sA, float *sB,
-                                                  uint8_t *stage, const float4 *W, const float2 *W1) {
+                                                  uint8_t *stage, const float4 *W, const float2 *W1,
+                                                  int next = -1) {
     const int tid = threadIdx.x;
     const int m = (tid & 3) * 2;
+    // the next block's entry window, fetched early (used after the dequantisation)
+    uint64_t nbase = 0;
+    uint32_t nlines = 0;
+    if (next >= 0 && tid < 32) {
+        nbase = __ldg(P.base + next);
+        nlines = (min(entry_cap(__ldg(&P.items[next].len)), 512u) + 31) / 32;   // 128-byte lines
+    }
     const DecItem it = P.items[item];
     const EntHdr h = load_hdr<CG>(P.hdr + item);
     const uint64_t base = P.base[item];
@@ -692,6 +703,8 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         if ((tid & 31) == 0) atomicAdd(&s_l1, l1);
         __syncthreads();
         const bool fast = s_l1 < kFastL1;
+        if ((uint32_t)tid < nlines)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(P.arena + nbase + 32ull * tid));
         // pass 1: lines along x (cz,cy), box -> A[cz][cy][x]; the output pair
         // (m, m+1) of one line accumulates as one packed pair
         const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
@@ -818,11 +831,13 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
     for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
         const int j0 = 2 * pr, j1 = 2 * pr + 1;
         const int i0 = P.idx ? (int)P.idx[j0] : j0;
-        reconstruct_block<false>(P, i0, sA, sB, sStage0, sW, sW1);
+        const int i1 = j1 < P.n ? (P.idx ? (int)P.idx[j1] : j1) : -1;
+        const int jn = 2 * (pr + gridDim.x);   // this CTA's next pair
+        const int in = jn < P.n ? (P.idx ? (int)P.idx[jn] : jn) : -1;
+        reconstruct_block<false>(P, i0, sA, sB, sStage0, sW, sW1, i1 >= 0 ? i1 : in);
         const DecItem a = P.items[i0];
-        if (j1 < P.n) {
-            const int i1 = P.idx ? (int)P.idx[j1] : j1;
-            reconstruct_block<false>(P, i1, sA, sB, sStage1, sW, sW1);
+        if (i1 >= 0) {
+            reconstruct_block<false>(P, i1, sA, sB, sStage1, sW, sW1, in);
             const DecItem b = P.items[i1];
             if (pairable(a, b)) {
                 uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
