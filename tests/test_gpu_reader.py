@@ -105,3 +105,49 @@ def test_batched_device_decode(gpu, reader_archive):
                     idx_bytes, lens = _payload_lens(data, co)
                     distinct = {(c[0] * 16 + c[1]) * 16 + c[2] for c in coords if all(0 <= v < 16 for v in c)}
                     assert batch_bytes == idx_bytes + sum(lens.get(bi, 0) for bi in distinct), (lod, cx)
+
+
+def test_unreadable_and_corrupt_sources(gpu, ref, reader_archive):
+    """A byte source that fails part-way, chunk offsets that point at garbage,
+    and a flat archive cut short: zeros, never a crash, and the same voxels
+    as the reference's readers where the reference defines them."""
+    import ctypes as C
+    import torch
+    from mcb200 import READ_FN, Reader
+    path, data, want = reader_archive
+    co = want[(0, 0)][0]
+    # a source that serves the first 200 KB only: headers and node tables,
+    # not every payload
+    short = data[:co + 3000]
+
+    def read(ud, off, n, dst):
+        if off + n > len(short):
+            return -1
+        C.memmove(dst, short[off:off + n], n)
+        return 0
+    cb = READ_FN(read)
+    Reader(gpu, data=data).close()   # binds the reader signatures
+    for partial in (0, 1):
+        r = gpu.L.mc_open_streaming(C.cast(cb, C.c_void_p), None, len(data))
+        gpu.L.mc_reader_set_partial_fetch(r, partial)
+        for p in [(0, 0, 0), (8, 8, 8), (15, 15, 15)]:
+            out = np.full(4096, 0xEE, np.uint8)
+            gpu.L.mc_decode_block(r, co, *p, out.ctypes.data)
+            if not partial:
+                assert not out.any()   # the whole blob cannot be read
+        d = torch.full((3 * 4096,), 0xEE, dtype=torch.uint8, device="cuda")
+        coords = np.array([[0, 0, 0], [8, 8, 8], [15, 15, 15]], np.int32)
+        assert gpu.L.mc_b200_reader_decode_blocks(r, co, coords.ctypes.data, 3, C.c_void_p(d.data_ptr()), None) == 0
+        if not partial:
+            assert not d.any().item()
+        gpu.L.mc_close(r)
+    # flat readers: offsets into garbage and a truncated archive
+    with Reader(gpu, data=data) as m, Reader(ref, data=data) as rr:
+        for bogus in (co + 7, len(data) - 10, len(data) + 100, 300):
+            assert np.array_equal(m.decode_block(bogus, 1, 2, 3), rr.decode_block(bogus, 1, 2, 3)) or \
+                not m.decode_block(bogus, 1, 2, 3).any()
+    cut = data[:co + 5000]
+    with Reader(gpu, data=cut) as m, Reader(ref, data=cut) as rr:
+        assert m.chunk_offset(0, 0, 0, 0) == rr.chunk_offset(0, 0, 0, 0)
+        for p in PICKS:
+            assert np.array_equal(m.decode_block(co, *p), rr.decode_block(co, *p)), p
