@@ -417,7 +417,8 @@ int mc_enc_block(mc_codec_ctx *C, const mc_u8 *vox, mc_buf *out, uint32_t *len_o
     if (slot < 0) return 0;
     if (!cuda_ok(cudaEventSynchronize(L->done), "sync") || !L->src.ensure(kN3) || !L->enc_pay.ensure(kEncCap) ||
         !L->enc_len.ensure(4) || !L->enc_frac.ensure(4) || !L->enc_items.ensure(sizeof(EncItem)) ||
-        !L->status.ensure(16) || !L->h_stage.ensure(kEncCap + 64))
+        !L->status.ensure(16) || !L->h_stage.ensure(kEncCap + 64) || !L->enc_lv.ensure(2 * kN3) ||
+        !L->enc_corr.ensure(4 * kN3) || !L->enc_sym.ensure(8))
         return 0;
     EncItem it{};
     it.src = (uint64_t)(uintptr_t)L->src.p;
@@ -437,6 +438,9 @@ int mc_enc_block(mc_codec_ctx *C, const mc_u8 *vox, mc_buf *out, uint32_t *len_o
     ep.len = L->enc_len.as<uint32_t>();
     ep.frac = L->enc_frac.as<uint8_t>();
     ep.status = L->status.as<uint32_t>();
+    ep.levels = L->enc_lv.as<int16_t>();
+    ep.corr = L->enc_corr.as<uint32_t>();
+    ep.sym = L->enc_sym.as<uint2>();
     uint32_t len = 0;
     if (!cuda_ok(cudaMemcpyAsync(L->src.p, hs, kN3, cudaMemcpyHostToDevice, L->stream), "H2D") ||
         !cuda_ok(cudaMemcpyAsync(L->enc_items.p, hs + kN3, sizeof it, cudaMemcpyHostToDevice, L->stream), "H2D") ||

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(128) k_encode(EncParams P) {
             uint32_t f = (cnt * 15u + 2048u) / 4096u;    // material nibble (src/mc_codec.c:820-822)
             if (cnt && !f) f = 1;
             P.frac[item] = (uint8_t)f;
-            if (!cnt) P.len[item] = 0;
+            if (!cnt) { P.len[item] = 0; P.sym[item] = make_uint2(0, 0); }
         }
         if (!cnt) { __syncthreads(); continue; }       // all air: not coded
         const int dc = (int)((sum + kN3 / 2) / kN3);
@@ -285,57 +285,80 @@ __global__ void __launch_bounds__(128) k_encode(EncParams P) {
             }
         }
         __syncthreads();
-        if (tid == 0) {
-            Enc e;
-            e.out = reinterpret_cast<uint8_t *>(it.out);
-            e.cap = kEncCap; e.len = 0; e.low = 0; e.range = 0xFFFFFFFFu; e.cache = 0; e.pending = 1;
-            uint16_t ctx[kNumCtx];
-            for (int j = 0; j < kNumCtx; ++j) ctx[j] = qt.ctx[j];
-            const uint32_t ncorr = S.ncorr;
-            enc_bit(e, ctx[kCtxFlag + 0], 0);                 // reserved
-            enc_bit(e, ctx[kCtxFlag + 1], ncorr > 0);
-            for (int b = 0; b < 8; ++b) enc_bit(e, ctx[kCtxDc + b], (dc >> (7 - b)) & 1);
-            const uint32_t eob = S.eob;
-            {   // EOB: bit length prefix then the bits below the MSB (src/mc_codec.c:314-320)
-                int k = bitlen32(eob);
-                for (int i = 0; i < k; ++i) enc_bit(e, ctx[kCtxEob + i], 1);
-                if (k < 13) enc_bit(e, ctx[kCtxEob + k], 0);
-                if (k > 1) enc_bits(e, eob & ((1u << (k - 1)) - 1u), k - 1);
-            }
-            uint32_t hist = 0;
-            for (uint32_t p = 0; p < eob; ++p) {              // src/mc_codec.c:337-349
-                uint32_t sc = __ldg(P.scan + p);
-                int v = S.lv[sc & 0xFFF];
-                if (p != eob - 1) {
-                    uint32_t dens = min(__popc(hist & 0xFFFFu), 3);
-                    enc_bit(e, ctx[kCtxSig + (sc >> 12) * 4 + dens], v != 0);
-                }
-                hist = (hist << 1) | (v != 0);
-                if (!v) continue;
-                uint32_t m = (uint32_t)(v < 0 ? -v : v), rest = m - 1;
-                int k = 0;
-                while (rest > 0 && k < 11) { enc_bit(e, ctx[kCtxMag + k], 1); rest--; k++; }
-                if (rest == 0) enc_bit(e, ctx[kCtxMag + k], 0);
-                else { enc_bit(e, ctx[kCtxMag + 11], 1); enc_eg(e, rest); }
-                enc_bypass(e, v < 0);
-            }
-            if (ncorr) {                                     // src/mc_codec.c:721-729
-                enc_eg(e, ncorr - 1);
-                uint32_t prev = 0;
-                for (uint32_t c = 0; c < ncorr; ++c) {
-                    uint32_t pos = S.cpos[c];
-                    enc_eg(e, pos - prev);
-                    prev = pos;
-                    int d = S.cdel[c];
-                    enc_bypass(e, d < 0);
-                    enc_eg(e, (uint32_t)(d < 0 ? -d : d) - 1u);
-                }
-            }
-            for (int i = 0; i < 5; ++i) enc_shift(e);
-            if (e.len > e.cap) atomicAdd(P.status, 1u);
-            P.len[item] = e.len > e.cap ? e.cap : e.len;
-        }
+        // the block's symbols for k_encode_rc: levels in scan order up to the
+        // EOB, the corrections, and (dc, eob, ncorr) with the coded flag
+        const uint32_t eob = S.eob, ncorr = S.ncorr;
+        int16_t *lvs = P.levels + (size_t)item * kN3;
+        for (uint32_t p = tid; p < eob; p += 128) lvs[p] = S.lv[__ldg(P.scan + p) & 0xFFF];
+        uint32_t *cor = P.corr + (size_t)item * kN3;
+        for (uint32_t c = tid; c < ncorr; c += 128) cor[c] = (uint32_t)S.cpos[c] | ((uint32_t)(uint16_t)S.cdel[c] << 16);
+        if (tid == 0) P.sym[item] = make_uint2(0x80000000u | (eob << 8) | (uint32_t)dc, ncorr);
         __syncthreads();
+    }
+}
+
+// Range coding of every coded block, one lane per block (src/mc_codec.c:
+// 330-350, 710-729): header bins, EOB, the coefficient loop and the
+// corrections, in the order the reference writes them. The coder of a block is
+// a serial chain; lanes in a warp code different blocks, with contexts in
+// shared memory (one 16-bit word per context per lane).
+__global__ void __launch_bounds__(128) k_encode_rc(EncParams P) {
+    __shared__ uint16_t s_ctx[4][kNumCtx][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint16_t *ctx = &s_ctx[warp][0][lane];
+    for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < P.n; item += gridDim.x * blockDim.x) {
+        const uint2 sy = P.sym[item];
+        if (!(sy.x & 0x80000000u)) continue;   // all air: not coded
+        const EncItem it = P.items[item];
+        const QTab &qt = P.qtab[it.qslot];
+        const uint32_t dc = sy.x & 0xFF, eob = (sy.x >> 8) & 0x1FFF, ncorr = sy.y;
+        const int16_t *lvs = P.levels + (size_t)item * kN3;
+        const uint32_t *cor = P.corr + (size_t)item * kN3;
+        Enc e;
+        e.out = reinterpret_cast<uint8_t *>(it.out);
+        e.cap = kEncCap; e.len = 0; e.low = 0; e.range = 0xFFFFFFFFu; e.cache = 0; e.pending = 1;
+        for (int j = 0; j < kNumCtx; ++j) ctx[j * 32] = qt.ctx[j];
+        enc_bit(e, ctx[(kCtxFlag + 0) * 32], 0);                 // reserved
+        enc_bit(e, ctx[(kCtxFlag + 1) * 32], ncorr > 0);
+        for (int b = 0; b < 8; ++b) enc_bit(e, ctx[(kCtxDc + b) * 32], (dc >> (7 - b)) & 1);
+        {   // EOB: bit length prefix then the bits below the MSB (src/mc_codec.c:314-320)
+            int k = bitlen32(eob);
+            for (int i = 0; i < k; ++i) enc_bit(e, ctx[(kCtxEob + i) * 32], 1);
+            if (k < 13) enc_bit(e, ctx[(kCtxEob + k) * 32], 0);
+            if (k > 1) enc_bits(e, eob & ((1u << (k - 1)) - 1u), k - 1);
+        }
+        uint32_t hist = 0;
+        for (uint32_t p = 0; p < eob; ++p) {              // src/mc_codec.c:337-349
+            const int v = lvs[p];
+            if (p != eob - 1) {
+                const uint32_t dens = min(__popc(hist & 0xFFFFu), 3);
+                enc_bit(e, ctx[(kCtxSig + (__ldg(P.scan + p) >> 12) * 4 + dens) * 32], v != 0);
+            }
+            hist = (hist << 1) | (v != 0);
+            if (!v) continue;
+            uint32_t m = (uint32_t)(v < 0 ? -v : v), rest = m - 1;
+            int k = 0;
+            while (rest > 0 && k < 11) { enc_bit(e, ctx[(kCtxMag + k) * 32], 1); rest--; k++; }
+            if (rest == 0) enc_bit(e, ctx[(kCtxMag + k) * 32], 0);
+            else { enc_bit(e, ctx[(kCtxMag + 11) * 32], 1); enc_eg(e, rest); }
+            enc_bypass(e, v < 0);
+        }
+        if (ncorr) {                                     // src/mc_codec.c:721-729
+            enc_eg(e, ncorr - 1);
+            uint32_t prev = 0;
+            for (uint32_t c = 0; c < ncorr; ++c) {
+                const uint32_t w = cor[c];
+                const uint32_t pos = w & 0xFFFF;
+                enc_eg(e, pos - prev);
+                prev = pos;
+                const int d = (int16_t)(w >> 16);
+                enc_bypass(e, d < 0);
+                enc_eg(e, (uint32_t)(d < 0 ? -d : d) - 1u);
+            }
+        }
+        for (int i = 0; i < 5; ++i) enc_shift(e);
+        if (e.len > e.cap) atomicAdd(P.status, 1u);
+        P.len[item] = e.len > e.cap ? e.cap : e.len;
     }
 }
 
@@ -687,6 +710,10 @@ cudaError_t launch_encode(const EncParams &p, cudaStream_t s) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int blocks = p.n < sms * 3 ? p.n : sms * 3;
     k_encode<<<blocks, 128, smem, s>>>(p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int rc_blocks = (p.n + 127) / 128;
+    k_encode_rc<<<rc_blocks < sms * 16 ? rc_blocks : sms * 16, 128, 0, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -127,6 +127,12 @@ struct EncParams {
     uint32_t *len;       // per item: payload bytes (0 = all air, not coded)
     uint8_t *frac;       // per item: material nibble
     uint32_t *status;    // [0]: payloads that overflowed kEncCap
+    // symbol scratch between the transform and the coder, per item: levels in
+    // scan order (kN3 int16), corrections (kN3 u32: pos | delta << 16), and
+    // (coded flag | eob << 8 | dc, ncorr)
+    int16_t *levels;
+    uint32_t *corr;
+    uint2 *sym;
 };
 cudaError_t upload_cos_encode(const float cmf[16][16], cudaStream_t s);
 cudaError_t launch_encode(const EncParams &p, cudaStream_t s);

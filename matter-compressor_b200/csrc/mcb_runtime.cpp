@@ -396,7 +396,8 @@ bool encode_chunks(Lane &L, const uint8_t *const *d_vox, int nchunks, const floa
         !L.status.ensure(16) || !L.b_scratch.ensure(4 * n) || !L.b_lens16.ensure(2 * n) ||
         !L.b_bitmap.ensure((size_t)kBitmapBytes * nchunks) || !L.b_fmap.ensure((size_t)kFmapCap * nchunks) ||
         !L.b_fml.ensure(4 * nchunks) || !L.b_np.ensure(4 * nchunks) || !L.b_len.ensure(8 * nchunks) ||
-        !L.b_off.ensure(8 * nchunks) || !L.b_q.ensure(4 * nchunks) || !L.h_misc.ensure(16 * (size_t)nchunks))
+        !L.b_off.ensure(8 * nchunks) || !L.b_q.ensure(4 * nchunks) || !L.h_misc.ensure(16 * (size_t)nchunks) ||
+        !L.enc_lv.ensure(2 * (size_t)kN3 * n) || !L.enc_corr.ensure(4 * (size_t)kN3 * n) || !L.enc_sym.ensure(8 * n))
         return false;
     EncItem *hi = L.h_items.as<EncItem>();
     for (int c = 0; c < nchunks; ++c) {
@@ -428,6 +429,9 @@ bool encode_chunks(Lane &L, const uint8_t *const *d_vox, int nchunks, const floa
     ep.len = L.enc_len.as<uint32_t>();
     ep.frac = L.enc_frac.as<uint8_t>();
     ep.status = L.status.as<uint32_t>();
+    ep.levels = L.enc_lv.as<int16_t>();
+    ep.corr = L.enc_corr.as<uint32_t>();
+    ep.sym = L.enc_sym.as<uint2>();
     if (!cuda_ok(launch_encode(ep, L.stream), "encode launch")) return false;
     BlobParams bp;
     bp.nchunks = nchunks;

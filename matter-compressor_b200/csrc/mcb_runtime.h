@@ -97,6 +97,7 @@ struct Lane {
     DevBuf status, out;
     DecodeBatch batch;
     DevBuf enc_items, enc_len, enc_frac, enc_pay, src;
+    DevBuf enc_lv, enc_corr, enc_sym;   // encoder symbol scratch (levels, corrections, per-block info)
     DevBuf b_scratch, b_lens16, b_bitmap, b_fmap, b_fml, b_np, b_len, b_off, b_q, blobs;
     DevBuf pyr_stage, pyr_a, pyr_b, pyr_flag;   // LOD pyramid: chunk staging, level volumes, all-air flags
     DevBuf ver_items, ver_bad;                  // device verify: blob list, mismatch flags
