@@ -659,12 +659,43 @@ def run_encode(args):
         t = statistics.median(times[1:]) if len(times) > 1 else times[0]
         rows.append({"level": lvl, "q": q, "tau": tau, "gbs": round(8 * CHUNK / t / 1e9, 3), "ms": round(t * 1e3, 2),
                      "archive_bytes": size})
+    # the reference's own encode of the same chunks at preset 4 (q=6, tau=16):
+    # its ctx path (one thread) and its parallel path (all threads, no tau)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import REF_FAST_LIB
+        try:
+            ref = McLib(REF_FAST_LIB, b200=False)
+            ref.L.mc_codec_init()
+            host = [v.cpu().numpy() for v in vox[:2]]
+            res = {}
+            for mode in ("ctx", "par"):
+                path = os.path.join(td, f"ref_{mode}.mca")
+                with ref.open(path, 256 * 8, 256, 256, 6.0) as a:
+                    c = ref.ctx(6.0, 16)
+                    t0 = time.perf_counter()
+                    for i, h in enumerate(host):
+                        if mode == "ctx":
+                            assert ref.L.mc_archive_append_chunk_ctx(a.a, c, 0, 0, 0, i, h.ctypes.data) == 0
+                        else:
+                            assert ref.L.mc_archive_append_chunk_par(a.a, 0, 0, 0, i, h.ctypes.data, 6.0, 0) == 0
+                    res[mode] = len(host) * CHUNK / (time.perf_counter() - t0) / 1e9
+                    ref.L.mc_codec_ctx_free(c)
+                os.remove(path)
+            cpu = {"value": round(res["ctx"], 4), "unit": "GB/s", "cores": 1, "kind": "reference",
+                   "sample": "the reference's mc_archive_append_chunk_ctx at preset 4 (q=6, tau=16) on 2 of the "
+                             "same chunks, default-flag build",
+                   "parallel_path_gbs": round(res["par"], 4),
+                   "parallel_path": f"mc_archive_append_chunk_par(nthreads=0, q=6, no tau) on {os.cpu_count()} "
+                                    "host threads"}
+        except (FileNotFoundError, OSError) as e:
+            cpu = {"value": None, "sample": f"unavailable: {e}"}
     os.rmdir(td)
     return {"metric": "preset-ladder batched encode: raw GB/s per level (8 x 256^3, 30% air)",
             "workload": "encode", "unit": "GB/s", "n_gpus": 1, "dtype": "u8", "data": "synthetic",
             "config": {"workload": "mc_b200_append_chunks of 8 chunks per preset level (q, tau from the preset "
                                    "table), host timing around the call (encode, blob assembly, install)"},
-            "levels": rows, "tau_bound_holds": worst <= 0}
+            "levels": rows, "tau_bound_holds": worst <= 0, "cpu_baseline": cpu}
 
 # ------------------------------------------------------------------ arms
 def run_reference(args, d):
