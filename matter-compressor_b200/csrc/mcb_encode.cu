@@ -481,93 +481,8 @@ __device__ __forceinline__ uint64_t ld64u(const uint8_t *p) {
     for (int i = 7; i >= 0; --i) v = (v << 8) | p[i];
     return v;
 }
-__device__ __forceinline__ uint32_t ld32u(const uint8_t *p) {
-    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
-}
 
-// Stripe loader: bytes one at a time (any address).
-struct ByteLoad {
-    __device__ uint64_t operator()(const uint8_t *p) const { return ld64u(p); }
-};
-
-// XXH64 computed by 4 cooperating lanes (lanes 0..3 of a warp): lane i owns
-// accumulator i over the 32-byte stripes; lane 0 merges and hashes the tail.
-// Returns the hash in every participating lane.
-template <class LD = ByteLoad>
-__device__ uint64_t xxh64_4(const uint8_t *p, uint64_t len, uint64_t seed, int lane, unsigned gm, LD ld = LD()) {
-    uint64_t h = 0;
-    const uint64_t nstripes = len >= 32 ? len / 32 : 0;
-    uint64_t acc = 0;
-    if (nstripes) {
-        acc = lane == 0 ? seed + XP1 + XP2 : lane == 1 ? seed + XP2 : lane == 2 ? seed : seed - XP1;
-        const uint8_t *q = p + 8 * lane;
-        // Batches of 8 stripes, double-buffered in registers: the loads of the
-        // next batch are in flight while this batch's rounds (a serial chain)
-        // run, so a lane waits on memory once per stream, not once per batch.
-        constexpr int K = 8;
-        uint64_t s = 0;
-        if (nstripes >= K) {
-            uint64_t cur[K], nxt[K];
-#pragma unroll
-            for (int j = 0; j < K; ++j) cur[j] = ld(q + 32 * j);
-            for (; s + 2 * K <= nstripes; s += K) {
-#pragma unroll
-                for (int j = 0; j < K; ++j) nxt[j] = ld(q + 32 * (s + K + j));
-#pragma unroll
-                for (int j = 0; j < K; ++j) acc = xround(acc, cur[j]);
-#pragma unroll
-                for (int j = 0; j < K; ++j) cur[j] = nxt[j];
-            }
-#pragma unroll
-            for (int j = 0; j < K; ++j) acc = xround(acc, cur[j]);
-            s += K;
-        }
-        for (; s < nstripes; ++s) acc = xround(acc, ld(q + 32 * s));
-    }
-    uint64_t a0 = __shfl_sync(gm, acc, 0, 4), a1 = __shfl_sync(gm, acc, 1, 4);
-    uint64_t a2 = __shfl_sync(gm, acc, 2, 4), a3 = __shfl_sync(gm, acc, 3, 4);
-    if (lane == 0) {
-        if (nstripes) {
-            h = rotl64(a0, 1) + rotl64(a1, 7) + rotl64(a2, 12) + rotl64(a3, 18);
-            h = (h ^ xround(0, a0)) * XP1 + XP4;
-            h = (h ^ xround(0, a1)) * XP1 + XP4;
-            h = (h ^ xround(0, a2)) * XP1 + XP4;
-            h = (h ^ xround(0, a3)) * XP1 + XP4;
-        } else {
-            h = seed + XP5;
-        }
-        h += len;
-        const uint8_t *t = p + nstripes * 32, *end = p + len;
-        for (; end - t >= 8; t += 8) h = rotl64(h ^ xround(0, ld64u(t)), 27) * XP1 + XP4;
-        if (end - t >= 4) { h = rotl64(h ^ ((uint64_t)ld32u(t) * XP1), 23) * XP2 + XP3; t += 4; }
-        for (; t < end; ++t) h = rotl64(h ^ ((uint64_t)*t * XP5), 11) * XP1;
-        h ^= h >> 33; h *= XP2; h ^= h >> 29; h *= XP3; h ^= h >> 32;
-    }
-    return __shfl_sync(gm, h, 0, 4);
-}
 }  // namespace
-
-// Hash chain per chunk, 4 lanes per chunk (src/mc_archive.c:76-88).
-__global__ void k_blob_hash(BlobParams P) {
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
-    const int lane = threadIdx.x & 3;
-    const unsigned gm = 0xFu << ((threadIdx.x & 31) & ~3);
-    if (c >= P.nchunks) return;   // whole 4-lane groups leave together
-    const uint64_t total = P.blob_len[c];
-    if (!total) return;
-    uint8_t *blob = P.blobs + P.blob_off[c];
-    uint16_t fml = (uint16_t)(blob[12] | (blob[13] << 8));
-    const uint8_t *fmap = blob + kBlobHdr, *bm = fmap + fml, *lens = bm + kBitmapBytes;
-    const uint32_t np = P.np[c];
-    const uint64_t pay = (uint64_t)kBlobHdr + fml + kBitmapBytes + 2ull * np;
-    uint64_t h = xxh64_4(fmap, fml, kHashSeed, lane, gm);
-    h ^= xxh64_4(bm, kBitmapBytes, h, lane, gm);
-    h ^= xxh64_4(lens, 2ull * np, h, lane, gm);
-    h ^= xxh64_4(blob + pay, total - pay, h, lane, gm);
-    if (lane == 0) {
-        for (int i = 0; i < 8; ++i) blob[4 + i] = (uint8_t)(h >> (8 * i));
-    }
-}
 
 // Device verify (src/mc_archive.c:1072-1111): the chained hash of every
 // listed blob of an archive held in device memory, compared with the hash
@@ -684,6 +599,31 @@ __global__ void __launch_bounds__(kVerifyWarps * 32) k_verify_hash(const uint8_t
     if ((threadIdx.x & 31) == 0) bad[c] = h != ld64u(blob + 4) ? 1u : 0u;
 }
 
+// Hash chain per chunk blob (src/mc_archive.c:76-88), one warp per blob
+// through the same shared-memory tiles as the verify kernel; the hash goes
+// into the blob header.
+__global__ void __launch_bounds__(kVerifyWarps * 32) k_blob_hash(BlobParams P) {
+    __shared__ __align__(16) uint8_t s_tile[kVerifyWarps][kTileBuf];
+    const int w = threadIdx.x >> 5;
+    const int c = blockIdx.x * kVerifyWarps + w;
+    if (c >= P.nchunks) return;   // whole warps leave together
+    const uint64_t total = P.blob_len[c];
+    if (!total) return;
+    uint8_t *tile = s_tile[w];
+    uint8_t *blob = P.blobs + P.blob_off[c];
+    const uint8_t *limit = blob + total;
+    const uint16_t fml = (uint16_t)(blob[12] | (blob[13] << 8));
+    const uint8_t *fmap = blob + kBlobHdr, *bm = fmap + fml, *lens = bm + kBitmapBytes;
+    const uint32_t np = P.np[c];
+    const uint64_t pay = (uint64_t)kBlobHdr + fml + kBitmapBytes + 2ull * np;
+    uint64_t h = xxh64_warp(blob, limit, fmap, fml, kHashSeed, tile);
+    h ^= xxh64_warp(blob, limit, bm, kBitmapBytes, h, tile);
+    h ^= xxh64_warp(blob, limit, lens, 2ull * np, h, tile);
+    h ^= xxh64_warp(blob, limit, blob + pay, total - pay, h, tile);
+    if ((threadIdx.x & 31) == 0)
+        for (int i = 0; i < 8; ++i) blob[4 + i] = (uint8_t)(h >> (8 * i));
+}
+
 cudaError_t launch_verify_hash(const uint8_t *d_arc, uint64_t arc_len, const VerifyItem *d_items, int n,
                                uint32_t *d_bad, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
@@ -729,8 +669,7 @@ cudaError_t launch_blob_fill(const BlobParams &p, cudaStream_t s) {
 }
 cudaError_t launch_blob_hash(const BlobParams &p, cudaStream_t s) {
     if (p.nchunks <= 0) return cudaSuccess;
-    int threads = p.nchunks * 4;
-    k_blob_hash<<<(threads + 127) / 128, 128, 0, s>>>(p);
+    k_blob_hash<<<(p.nchunks + kVerifyWarps - 1) / kVerifyWarps, kVerifyWarps * 32, 0, s>>>(p);
     return cudaGetLastError();
 }
 
