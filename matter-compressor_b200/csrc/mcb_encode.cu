@@ -167,9 +167,8 @@ struct EncSmem {
     float a[kN3];
     float b[kN3];
     int16_t lv[kN3];
-    uint16_t cpos[kN3];
-    int16_t cdel[kN3];
     uint8_t vox[kN3];
+    uint32_t mask[4][32];   // max-error pass: hit masks per warp and step
     uint32_t red[8];
     uint32_t ncorr;
     uint32_t eob;
@@ -259,39 +258,51 @@ __global__ void __launch_bounds__(128) k_encode(EncParams P) {
             }
             __syncthreads();
             transform3<false>(S.a, S.b);                 // reconstruction in S.b
-            // corrections in ascending voxel order: warp w scans rows of 32
+            // corrections in ascending voxel order, written straight to the
+            // coder's scratch: warp w owns voxels [1024w, 1024w + 1024) in 32
+            // steps of 32; a first pass counts its hits (the step masks kept
+            // in shared memory), one barrier gives every warp its start, and a
+            // second pass writes the entries
             const int lane = tid & 31, w = tid >> 5;
-            for (int base = 0; base < kN3; base += 128) {
-                int i = base + tid;
+            auto hit_at = [&](int i, int &dl) {
                 long long rr = __float2ll_rn(S.b[i]);
                 int v = (int)(uint32_t)(unsigned long long)rr + dc;
                 v = v < 0 ? 0 : v > 255 ? 255 : v;
-                int err = (int)S.vox[i] - v;
-                int ae = err < 0 ? -err : err;
-                bool hit = ae > (int)it.tau;
-                uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-                if (lane == 0) S.red[w] = __popc(m);
-                __syncthreads();
-                uint32_t before = S.ncorr;
-                for (int ww = 0; ww < w; ++ww) before += S.red[ww];
-                if (hit) {
-                    uint32_t slot = before + __popc(m & ((1u << lane) - 1u));
-                    S.cpos[slot] = (uint16_t)i;
-                    S.cdel[slot] = (int16_t)(err < 0 ? -(ae - (int)it.tau) : (ae - (int)it.tau));
-                }
-                __syncthreads();
-                if (tid == 0) S.ncorr += S.red[0] + S.red[1] + S.red[2] + S.red[3];
-                __syncthreads();
+                const int err = (int)S.vox[i] - v;
+                const int ae = err < 0 ? -err : err;
+                dl = err < 0 ? -(ae - (int)it.tau) : (ae - (int)it.tau);
+                return ae > (int)it.tau;
+            };
+            uint32_t cnt_w = 0;
+            for (int k = 0; k < 32; ++k) {
+                int dl;
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, hit_at(1024 * w + 32 * k + lane, dl));
+                if (lane == 0) S.mask[w][k] = m;
+                cnt_w += __popc(m);
             }
+            if (lane == 0) S.red[w] = cnt_w;
+            __syncthreads();
+            uint32_t at = 0;
+            for (int ww = 0; ww < w; ++ww) at += S.red[ww];
+            uint32_t *cor = P.corr + (size_t)item * kN3;
+            for (int k = 0; k < 32; ++k) {
+                const uint32_t m = S.mask[w][k];
+                if ((m >> lane) & 1) {
+                    int dl;
+                    const int i = 1024 * w + 32 * k + lane;
+                    hit_at(i, dl);
+                    cor[at + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i | ((uint32_t)(uint16_t)(int16_t)dl << 16);
+                }
+                at += __popc(m);
+            }
+            if (tid == 0) S.ncorr = S.red[0] + S.red[1] + S.red[2] + S.red[3];
         }
-        __syncthreads();
+        __syncthreads();   // eob (per-warp atomics) and ncorr complete
         // the block's symbols for k_encode_rc: levels in scan order up to the
         // EOB, the corrections, and (dc, eob, ncorr) with the coded flag
         const uint32_t eob = S.eob, ncorr = S.ncorr;
         int16_t *lvs = P.levels + (size_t)item * kN3;
         for (uint32_t p = tid; p < eob; p += 128) lvs[p] = S.lv[__ldg(P.scan + p) & 0xFFF];
-        uint32_t *cor = P.corr + (size_t)item * kN3;
-        for (uint32_t c = tid; c < ncorr; c += 128) cor[c] = (uint32_t)S.cpos[c] | ((uint32_t)(uint16_t)S.cdel[c] << 16);
         if (tid == 0) P.sym[item] = make_uint2(0x80000000u | (eob << 8) | (uint32_t)dc, ncorr);
         __syncthreads();
     }
@@ -643,12 +654,15 @@ cudaError_t launch_encode(const EncParams &p, cudaStream_t s) {
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_encode, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
         attr = true;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = p.n < sms * 3 ? p.n : sms * 3;
+    int blocks = p.n < sms * 5 ? p.n : sms * 5;   // 45.6 KB of shared memory: 5 CTAs per SM
     k_encode<<<blocks, 128, smem, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
