@@ -64,7 +64,8 @@ struct LaneState {
     const uint8_t *abase;      // payload start rounded down to 4 bytes
     uint32_t *ent;             // the block's entries in the arena (first cap of them)
     uint32_t len, off0;        // payload length, payload start - abase
-    uint32_t w, nxt, sel, jn;  // window word, next word, byte selector, index of the next word
+    uint32_t w, nxt, sel, jn;  // window word, next word (raw), byte selector, index of the next word
+    uint32_t nmask;            // the next word's payload bytes (applied when it enters the window)
     uint32_t code, range;
     uint32_t st, p, eob, hist, sigb, band, bend, stop, k, m;   // hist: significance flags, newest in bit 0
     uint32_t cc, pc;           // context slot of the next bin and its probability (coefficient loop)
@@ -77,20 +78,29 @@ struct LaneState {
 
 // Payload word j (bytes 4j-off0 .. 4j-off0+3 of the payload), bytes past the
 // payload read as zero (src/mc_codec.c:96). Loads are 4-byte aligned and never
-// start past the word holding the payload's last byte.
-__device__ __forceinline__ uint32_t load_word(const LaneState &L, uint32_t j) {
-    const int first = (int)(4 * j) - (int)L.off0;   // payload index of the word's byte 0
-    if (first >= (int)L.len) return 0u;
-    uint32_t v = __ldg(reinterpret_cast<const uint32_t *>(L.abase) + j);
-    const int avail = (int)L.len - first;
-    if (avail < 4) v &= (1u << (8 * avail)) - 1u;
+// start past the word holding the payload's last byte. The raw load and the
+// mask of its payload bytes are kept apart: the next word is loaded a refill
+// ahead and masked only when it enters the window, so nothing waits on the
+// load until then.
+__device__ __forceinline__ uint32_t word_mask(const LaneState &L, uint32_t j) {
+    const int avail = (int)L.len - ((int)(4 * j) - (int)L.off0);
+    return avail >= 4 ? 0xFFFFFFFFu : (avail <= 0 ? 0u : (1u << (8 * avail)) - 1u);
+}
+__device__ __forceinline__ uint32_t word_raw(const LaneState &L, uint32_t j) {
+    uint32_t v = 0;
+    if ((int)(4 * j) - (int)L.off0 < (int)L.len) v = __ldg(reinterpret_cast<const uint32_t *>(L.abase) + j);
     return v;
+}
+__device__ __forceinline__ uint32_t load_word(const LaneState &L, uint32_t j) {
+    return word_raw(L, j) & word_mask(L, j);
 }
 
 __device__ __forceinline__ void refill(LaneState &L) {
-    L.w = L.nxt;
+    L.w = L.nxt & L.nmask;
     L.sel = kSel0;
-    L.nxt = load_word(L, ++L.jn);
+    ++L.jn;
+    L.nmask = word_mask(L, L.jn);
+    L.nxt = word_raw(L, L.jn);
 }
 
 // One payload byte (slow paths). The window always holds an unread byte:
@@ -218,7 +228,8 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
     L.w = load_word(L, 0);
     L.sel = kSel0 + L.off0;
     L.jn = 1;
-    L.nxt = load_word(L, 1);
+    L.nmask = word_mask(L, 1);
+    L.nxt = word_raw(L, 1);
     L.range = 0xFFFFFFFFu;
     L.code = 0;
     for (int i = 0; i < 5; ++i) L.code = (L.code << 8) | next_byte(L);
