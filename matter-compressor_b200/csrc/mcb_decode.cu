@@ -947,7 +947,7 @@ __device__ __forceinline__ void reconstruct_pair(const RecParams &P, int j, floa
     }
 }
 
-__global__ void __launch_bounds__(128) k_decode_fused(FusedParams F) {
+__global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
     extern __shared__ __align__(16) uint8_t s_raw[];
     FusedSmem &S = *reinterpret_cast<FusedSmem *>(s_raw);
     const EntParams &P = F.e;
