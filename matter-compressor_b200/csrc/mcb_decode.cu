@@ -602,12 +602,36 @@ constexpr int kRowF = 20;            // A rows of 16 floats
 constexpr int kRowB = 16;            // B rows
 constexpr int kPlaneB = 16 * kRowB;  // one cz plane of B
 __device__ __forceinline__ int bswz(int y) { return (y >> 1) & 3; }
+// The coefficient box in B: coefficient (cz, cy, cx) at (cz*16 + cy)*17 + cx,
+// rows of 16 padded to 17 floats so that the 8 lines a warp reads in pass 1
+// sit in different banks. B holds kBoxB floats (the pass-2 output uses the
+// first 16 * kPlaneB).
+constexpr int kBoxRow = 17;
+constexpr int kBoxPlane = 16 * kBoxRow;
+constexpr int kBoxB = 16 * kBoxPlane;
 constexpr int kStageZ = 272;         // stage: one z slice of 16 rows of 16 bytes
 constexpr int kStageBytes = 16 * kStageZ;
+
+// Per-CTA state of the block being reconstructed: extents and L1 norm. Both
+// are zero when a block starts, like the coefficient box (rec_init, then
+// every block puts them back).
+__shared__ int s_rec_ext[3];
+__shared__ float s_rec_l1;
+
+// Before a CTA's first block: an all-zero coefficient box, zero extents and
+// L1 norm. The caller synchronises before the first block.
+__device__ __forceinline__ void rec_init(float *sB) {
+    for (int i = threadIdx.x; i < kBoxB / 4; i += blockDim.x)
+        reinterpret_cast<float4 *>(sB)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (threadIdx.x < 3) s_rec_ext[threadIdx.x] = 0;
+    if (threadIdx.x == 3) s_rec_l1 = 0.0f;
+}
 
 // Reconstruct one block into a stage (z slices of kStageZ bytes). Thread t owns the
 // output pair (m, m+1) = 2*(t&3) of every line it touches; its cosine weights
 // come from the shared table W.
+// On entry the coefficient box in sB, s_rec_ext and s_rec_l1 are zero; the
+// block leaves them zero again.
 // next: the item this CTA reconstructs after this one (-1: none). While this
 // block's transform runs, the start of the next block's entry list is
 // prefetched into L2, so that its loads do not wait on DRAM.
@@ -634,6 +658,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
     const int dc = it.len && sane ? h.dc : 0;
     const int nnz = it.len && sane ? h.nnz : 0;
     const int ncorr = it.len && sane ? h.ncorr : 0;
+    int E = 0;   // cz planes of the box this block wrote
 
     if (nnz == 0) {
         // constant block (src/mc_codec.c:757-759) or absent block (zeros)
@@ -641,87 +666,66 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         const uint4 v = make_uint4(w, w, w, w);
         for (int i = tid; i < kStageBytes / 16; i += 128) reinterpret_cast<uint4 *>(stage)[i] = v;
     } else {
-        // extents of the coefficient box: largest cz, cy, cx of any entry
-        // (src/mc_codec.c:371-372)
-        __shared__ int s_ext[3];
-        __shared__ float s_l1;
-        if (tid < 3) s_ext[tid] = 0;
-        if (tid == 3) s_l1 = 0.0f;
-        __syncthreads();
-        // A thread's first kKeep entries stay in registers for the
-        // dequantisation, as raster index | level << 16: blocks of up to
-        // 128 * kKeep entries read their entry list and scan table once.
-        constexpr int kKeep = 4;
-        uint32_t keep[kKeep];
+        // One pass over the entries: the extents of the coefficient box
+        // (largest cz, cy, cx of any entry, src/mc_codec.c:371-372), the
+        // dequantised coefficients (src/mc_codec_float.h:185-190) straight
+        // into the zeroed box, and the L1 norm. Four entries per thread are
+        // in flight at a time.
+        const QTab &qt = P.qtab[it.qslot];
         int mz = 0, my = 0, mx = 0;
+        float l1 = 0.0f;
+        for (int j0 = tid; j0 < nnz; j0 += 512) {
+            uint32_t e[4], ix[4];
 #pragma unroll
-        for (int k = 0; k < kKeep; ++k) {
-            const int j = tid + 128 * k;
-            uint32_t v = 0;
-            if (j < nnz) {
-                const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
-                const uint32_t idx = __ldg(P.scan + (e & 0xFFFu)) & 0xFFFu;
-                v = idx | (e & 0xFFFF0000u);
-                mz = max(mz, (int)((idx >> 8) & 15));
-                my = max(my, (int)((idx >> 4) & 15));
-                mx = max(mx, (int)(idx & 15));
+            for (int k = 0; k < 4; ++k) e[k] = j0 + 128 * k < nnz ? entry_at<CG>(P, base, cap, h.ovf, j0 + 128 * k) : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) ix[k] = j0 + 128 * k < nnz ? __ldg(P.scan + (e[k] & 0xFFFu)) & 0xFFFu : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (j0 + 128 * k >= nnz) break;
+                const int idx = (int)ix[k];
+                const int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;
+                mz = max(mz, cz);
+                my = max(my, cy);
+                mx = max(mx, cx);
+                const int lv = (int16_t)(e[k] >> 16);
+                if (lv) {
+                    const int f = cz + cy + cx;
+                    const float a = (float)(lv < 0 ? -lv : lv);
+                    const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
+                    sB[idx + (idx >> 4)] = lv < 0 ? -r : r;
+                    l1 = fadd(l1, r);
+                }
             }
-            keep[k] = v;
         }
-        for (int j = tid + 128 * kKeep; j < nnz; j += 128) {
-            const uint32_t e = __ldg(P.scan + (entry_at<CG>(P, base, cap, h.ovf, j) & 0xFFFu)) & 0xFFFu;
-            mz = max(mz, (int)((e >> 8) & 15));
-            my = max(my, (int)((e >> 4) & 15));
-            mx = max(mx, (int)(e & 15));
-        }
-        // one shared-memory atomic per warp
+        // one shared-memory atomic per warp and value; the L1 norm only
+        // bounds the voxels, so any summation order will do
         mz = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mz);
         my = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)my);
         mx = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mx);
-        if ((tid & 31) == 0) {
-            atomicMax(&s_ext[0], mz);
-            atomicMax(&s_ext[1], my);
-            atomicMax(&s_ext[2], mx);
-        }
-        __syncthreads();
-        const int E = s_ext[0] + 1, Y = s_ext[1] + 1, X = s_ext[2] + 1;
-        const QTab &qt = P.qtab[it.qslot];
-        for (int i = tid; i < E * Y * X; i += 128) sB[i] = 0.0f;
-        __syncthreads();
-        // dequantise (src/mc_codec_float.h:185-190) into box[cz][cy][cx]
-        float l1 = 0.0f;
-        auto dequant = [&](uint32_t v) {   // v: raster index | level << 16
-            const int idx = (int)(v & 0xFFFu);
-            const int lv = (int16_t)(v >> 16);
-            if (!lv) return;
-            const int cz = idx >> 8, cy = (idx >> 4) & 15, cx = idx & 15;
-            if (cz >= E || cy >= Y || cx >= X) return;
-            const int f = cz + cy + cx;
-            const float a = (float)(lv < 0 ? -lv : lv);
-            const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
-            sB[(cz * Y + cy) * X + cx] = lv < 0 ? -r : r;
-            l1 = fadd(l1, r);
-        };
-#pragma unroll
-        for (int k = 0; k < kKeep; ++k)
-            if (tid + 128 * k < nnz) dequant(keep[k]);
-        for (int j = tid + 128 * kKeep; j < nnz; j += 128) {
-            const uint32_t e = entry_at<CG>(P, base, cap, h.ovf, j);
-            dequant((__ldg(P.scan + (e & 0xFFFu)) & 0xFFFu) | (e & 0xFFFF0000u));
-        }
-        // the L1 norm only bounds the voxels: any summation order will do
         for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xFFFFFFFFu, l1, o);
-        if ((tid & 31) == 0) atomicAdd(&s_l1, l1);
+        if ((tid & 31) == 0) {
+            atomicMax(&s_rec_ext[0], mz);
+            atomicMax(&s_rec_ext[1], my);
+            atomicMax(&s_rec_ext[2], mx);
+            atomicAdd(&s_rec_l1, l1);
+        }
         __syncthreads();
-        const bool fast = s_l1 < kFastL1;
+        E = s_rec_ext[0] + 1;
+        const int Y = s_rec_ext[1] + 1, X = s_rec_ext[2] + 1;
+        const bool fast = s_rec_l1 < kFastL1;
         if ((uint32_t)tid < nlines)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(P.arena + nbase + 32ull * tid));
         // pass 1: lines along x (cz,cy), box -> A[cz][cy][x]; the output pair
-        // (m, m+1) of one line accumulates as one packed pair
+        // (m, m+1) of one line accumulates as one packed pair. Line l is
+        // (cz, cy) = (l / Y, l % Y); l < 256, so l * ceil(2^16 / Y) >> 16 is
+        // exactly l / Y.
         const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
+        const int invY = (65536 + Y - 1) / Y;
         for (int t = tid; t < E * Y * 4; t += 128) {
             const int line = t >> 2;
-            const float *in = sB + line * X;
+            const int cz = (line * invY) >> 16;
+            const float *in = sB + (cz * 16 + (line - cz * Y)) * kBoxRow;
             float2 e = make_float2(0.f, 0.f), o = e;
             int k = 0;
             for (; k + 1 < X; k += 2) {
@@ -741,6 +745,9 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             out[14 - m] = dif.y;
         }
         __syncthreads();
+        // every thread has read the extents and the norm: zero for the next block
+        if (tid < 3) s_rec_ext[tid] = 0;
+        if (tid == 3) s_rec_l1 = 0.0f;
         // pass 2: lines along y for 4 adjacent x at once, A[cz][k][x..x+3] -> B[cz][y][x..x+3]
         for (int t = tid; t < E * 16; t += 128) {
             const int xg = (t >> 2) & 3, cz = t >> 4;
@@ -780,6 +787,9 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         }
     }
     __syncthreads();
+    // the box planes this block wrote (coefficients and pass-2 output) back to zero
+    for (int i = tid; i < E * (kBoxPlane / 4); i += 128)
+        reinterpret_cast<float4 *>(sB)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (ncorr && tid == 0) {
         // corrections in stream order: a position may repeat, each
         // application clamps (src/mc_codec.c:775-781)
@@ -826,7 +836,7 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
     // sA: pass-1 output, then the second block's stage; sB: coefficient box,
     // then pass-2 output; sStage0: the first block's stage
     __shared__ __align__(16) float sA[16 * 16 * kRowF];
-    __shared__ __align__(16) float sB[16 * kPlaneB];
+    __shared__ __align__(16) float sB[kBoxB];
     __shared__ __align__(16) uint8_t sStage0[kStageBytes];
     __shared__ __align__(16) float4 sW[16 * 8];   // [k][m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}
     __shared__ __align__(8) float2 sW1[16 * 8];   // [k][m/2] = {c[k][m], c[k][m+1]}
@@ -836,6 +846,7 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
         sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
+    rec_init(sB);
     __syncthreads();
     const int tid = threadIdx.x;
     const int npairs = (P.n + 1) / 2;
@@ -892,7 +903,7 @@ struct FusedSmem {
         } e;
         struct {
             float A[16 * 16 * kRowF];
-            float B[16 * kPlaneB];
+            float B[kBoxB];
             uint8_t stage0[kStageBytes];
         } r;
     } u;
@@ -1002,6 +1013,8 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
         }
     }
     __syncthreads();   // the shared memory changes hands
+    rec_init(S.u.r.B);
+    __syncthreads();
 
     // ---- reconstruction over the completion list, one pair per claim
     const uint32_t npairs = ((uint32_t)F.r.n + 1u) >> 1;
@@ -1035,7 +1048,7 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
 // every pair is in the list.
 __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
     __shared__ __align__(16) float sA[16 * 16 * kRowF];
-    __shared__ __align__(16) float sB[16 * kPlaneB];
+    __shared__ __align__(16) float sB[kBoxB];
     __shared__ __align__(16) uint8_t sStage0[kStageBytes];
     __shared__ __align__(16) float4 sW[16 * 8];
     __shared__ __align__(8) float2 sW1[16 * 8];
@@ -1049,6 +1062,7 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
         sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
+    rec_init(sB);
     __syncthreads();
     for (uint32_t w = blockIdx.x; w < work; w += gridDim.x) {
         const uint32_t p = w < nsk ? F.ws[kFusedSkip0 + w] : claimed + (w - nsk);
