@@ -602,12 +602,12 @@ constexpr int kRowF = 20;            // A rows of 16 floats
 constexpr int kRowB = 16;            // B rows
 constexpr int kPlaneB = 16 * kRowB;  // one cz plane of B
 __device__ __forceinline__ int bswz(int y) { return (y >> 1) & 3; }
-// The coefficient box in B: coefficient (cz, cy, cx) at (cz*16 + cy)*17 + cx,
-// rows of 16 padded to 17 floats so that the 8 lines a warp reads in pass 1
-// sit in different banks. B holds kBoxB floats (the pass-2 output uses the
-// first 16 * kPlaneB).
-constexpr int kBoxRow = 17;
-constexpr int kBoxPlane = 16 * kBoxRow;
+// The coefficient box in B: coefficient (cz, cy, cx) at cz*kBoxPlane + cx*16 + cy.
+// For one (cz, cx) the 16 cy values are contiguous, so pass 1 reads the k-th
+// inputs of 4 adjacent x-lines as one float4; planes are padded by 16 floats
+// so that the two planes a warp reads sit in different banks. B holds kBoxB
+// floats (the pass-2 output uses the first 16 * kPlaneB).
+constexpr int kBoxPlane = 16 * 16 + 16;
 constexpr int kBoxB = 16 * kBoxPlane;
 constexpr int kStageZ = 272;         // stage: one z slice of 16 rows of 16 bytes
 constexpr int kStageBytes = 16 * kStageZ;
@@ -637,8 +637,7 @@ __device__ __forceinline__ void rec_init(float *sB) {
 // prefetched into L2, so that its loads do not wait on DRAM.
 template <bool CG>
 __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, float *sA, float *sB,
-                                                  uint8_t *stage, const float4 *W, const float2 *W1,
-                                                  int next = -1) {
+                                                  uint8_t *stage, const float4 *W, int next = -1) {
     const int tid = threadIdx.x;
     const int m = (tid & 3) * 2;
     // the next block's entry window, fetched early (used after the dequantisation)
@@ -693,7 +692,7 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
                     const int f = cz + cy + cx;
                     const float a = (float)(lv < 0 ? -lv : lv);
                     const float r = fadd(fadd(fmul(fsub(a, 1.0f), qt.step[f]), qt.dz8[f]), qt.dz4[f]);
-                    sB[idx + (idx >> 4)] = lv < 0 ? -r : r;
+                    sB[cz * kBoxPlane + cx * 16 + cy] = lv < 0 ? -r : r;
                     l1 = fadd(l1, r);
                 }
             }
@@ -716,33 +715,39 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         const bool fast = s_rec_l1 < kFastL1;
         if ((uint32_t)tid < nlines)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(P.arena + nbase + 32ull * tid));
-        // pass 1: lines along x (cz,cy), box -> A[cz][cy][x]; the output pair
-        // (m, m+1) of one line accumulates as one packed pair. Line l is
-        // (cz, cy) = (l / Y, l % Y); l < 256, so l * ceil(2^16 / Y) >> 16 is
-        // exactly l / Y.
+        // pass 1: lines along x for 4 adjacent cy at once, box[cz][k][cy..cy+3]
+        // -> A[cz*Y + cy][x]. Group g of plane cz holds lines cy = 4g..4g+3;
+        // lines at cy >= Y are zero and not stored. gi < 64, so
+        // gi * ceil(2^16 / G) >> 16 is exactly gi / G.
         const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
-        const int invY = (65536 + Y - 1) / Y;
-        for (int t = tid; t < E * Y * 4; t += 128) {
-            const int line = t >> 2;
-            const int cz = (line * invY) >> 16;
-            const float *in = sB + (cz * 16 + (line - cz * Y)) * kBoxRow;
-            float2 e = make_float2(0.f, 0.f), o = e;
-            int k = 0;
-            for (; k + 1 < X; k += 2) {
-                const float v = in[k], u = in[k + 1];
-                e = madd2(e, W1[k * 8 + mh], make_float2(v, v));
-                o = madd2(o, W1[(k + 1) * 8 + mh], make_float2(u, u));
+        const int G = (Y + 3) >> 2;
+        const int invG = (65536 + G - 1) / G;
+        for (int t = tid; t < E * G * 4; t += 128) {
+            const int gi = t >> 2;
+            const int cz = (gi * invG) >> 16;
+            const int cy0 = (gi - cz * G) << 2;
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + cz * kBoxPlane + cy0), 4, X, W, mh);
+            // line i of the group: outputs m, m+1 (e + o) and 15-m, 14-m (e - o)
+            const float2 p0 = add2(a.e0a, a.o0a), p1 = add2(a.e0b, a.o0b);
+            const float2 q0 = add2(a.e1a, a.o1a), q1 = add2(a.e1b, a.o1b);
+            const float2 r0 = sub2(a.e0a, a.o0a), r1 = sub2(a.e0b, a.o0b);
+            const float2 s0 = sub2(a.e1a, a.o1a), s1 = sub2(a.e1b, a.o1b);
+            float *out = sA + (cz * Y + cy0) * kRowF;
+            const int nl = min(Y - cy0, 4);
+            *reinterpret_cast<float2 *>(out + m) = make_float2(p0.x, q0.x);
+            *reinterpret_cast<float2 *>(out + 14 - m) = make_float2(s0.x, r0.x);
+            if (nl > 1) {
+                *reinterpret_cast<float2 *>(out + kRowF + m) = make_float2(p0.y, q0.y);
+                *reinterpret_cast<float2 *>(out + kRowF + 14 - m) = make_float2(s0.y, r0.y);
             }
-            if (k < X) {
-                const float v = in[k];
-                e = madd2(e, W1[k * 8 + mh], make_float2(v, v));
+            if (nl > 2) {
+                *reinterpret_cast<float2 *>(out + 2 * kRowF + m) = make_float2(p1.x, q1.x);
+                *reinterpret_cast<float2 *>(out + 2 * kRowF + 14 - m) = make_float2(s1.x, r1.x);
             }
-            const float2 sum = add2(e, o), dif = sub2(e, o);
-            float *out = sA + line * kRowF;
-            out[m] = sum.x;
-            out[m + 1] = sum.y;
-            out[15 - m] = dif.x;
-            out[14 - m] = dif.y;
+            if (nl > 3) {
+                *reinterpret_cast<float2 *>(out + 3 * kRowF + m) = make_float2(p1.y, q1.y);
+                *reinterpret_cast<float2 *>(out + 3 * kRowF + 14 - m) = make_float2(s1.y, r1.y);
+            }
         }
         __syncthreads();
         // every thread has read the extents and the norm: zero for the next block
@@ -839,12 +844,10 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
     __shared__ __align__(16) float sB[kBoxB];
     __shared__ __align__(16) uint8_t sStage0[kStageBytes];
     __shared__ __align__(16) float4 sW[16 * 8];   // [k][m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}
-    __shared__ __align__(8) float2 sW1[16 * 8];   // [k][m/2] = {c[k][m], c[k][m+1]}
     uint8_t *const sStage1 = reinterpret_cast<uint8_t *>(sA);
     for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
-        sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
     rec_init(sB);
     __syncthreads();
@@ -856,10 +859,10 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct(RecParams P) {
         const int i1 = j1 < P.n ? (P.idx ? (int)P.idx[j1] : j1) : -1;
         const int jn = 2 * (pr + gridDim.x);   // this CTA's next pair
         const int in = jn < P.n ? (P.idx ? (int)P.idx[jn] : jn) : -1;
-        reconstruct_block<false>(P, i0, sA, sB, sStage0, sW, sW1, i1 >= 0 ? i1 : in);
+        reconstruct_block<false>(P, i0, sA, sB, sStage0, sW, i1 >= 0 ? i1 : in);
         const DecItem a = P.items[i0];
         if (i1 >= 0) {
-            reconstruct_block<false>(P, i1, sA, sB, sStage1, sW, sW1, in);
+            reconstruct_block<false>(P, i1, sA, sB, sStage1, sW, in);
             const DecItem b = P.items[i1];
             if (pairable(a, b)) {
                 uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
@@ -908,7 +911,6 @@ struct FusedSmem {
         } r;
     } u;
     float4 W[16 * 8];
-    float2 W1[16 * 8];
     int pair;
 };
 
@@ -932,14 +934,14 @@ __device__ __forceinline__ int list_pair(const FusedParams &F, uint32_t p) {
 
 template <bool CG>
 __device__ __forceinline__ void reconstruct_pair(const RecParams &P, int j, float *sA, float *sB, uint8_t *stage0,
-                                                 const float4 *W, const float2 *W1) {
+                                                 const float4 *W) {
     const int tid = threadIdx.x;
     uint8_t *const stage1 = reinterpret_cast<uint8_t *>(sA);   // sA is free once a block is staged
     const int i0 = 2 * j, i1 = 2 * j + 1;
-    reconstruct_block<CG>(P, i0, sA, sB, stage0, W, W1);
+    reconstruct_block<CG>(P, i0, sA, sB, stage0, W);
     const DecItem a = P.items[i0];
     if (i1 < P.n) {
-        reconstruct_block<CG>(P, i1, sA, sB, stage1, W, W1);
+        reconstruct_block<CG>(P, i1, sA, sB, stage1, W);
         const DecItem b = P.items[i1];
         if (pairable(a, b)) {
             uint8_t *dst = reinterpret_cast<uint8_t *>(a.dst);
@@ -973,7 +975,6 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
     for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         S.W[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
-        S.W1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
     if (threadIdx.x == 0) { S.u.e.bend[7] = kN3; S.u.e.bend[8] = 0xFFFF; }
     __syncthreads();
@@ -1038,7 +1039,7 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
         __syncthreads();
         const int j = S.pair;
         if (j < 0) break;
-        reconstruct_pair<true>(F.r, j, S.u.r.A, S.u.r.B, S.u.r.stage0, S.W, S.W1);
+        reconstruct_pair<true>(F.r, j, S.u.r.A, S.u.r.B, S.u.r.stage0, S.W);
         __syncthreads();
     }
 }
@@ -1051,7 +1052,6 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
     __shared__ __align__(16) float sB[kBoxB];
     __shared__ __align__(16) uint8_t sStage0[kStageBytes];
     __shared__ __align__(16) float4 sW[16 * 8];
-    __shared__ __align__(8) float2 sW1[16 * 8];
     const uint32_t npairs = ((uint32_t)F.r.n + 1u) >> 1;
     const uint32_t claimed = min(F.ws[kFusedClaim], npairs);
     const uint32_t nsk = min(F.ws[kFusedNSkip], (uint32_t)kFusedMaxSkip);
@@ -1060,7 +1060,6 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
     for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
-        sW1[i] = make_float2(c_cos[k][mm], c_cos[k][mm + 1]);
     }
     rec_init(sB);
     __syncthreads();
@@ -1068,7 +1067,7 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
         const uint32_t p = w < nsk ? F.ws[kFusedSkip0 + w] : claimed + (w - nsk);
         const int j = p < npairs ? list_pair(F, p) : -1;
         if (j < 0 || (uint32_t)j >= npairs) continue;   // every pair is listed by now
-        reconstruct_pair<false>(F.r, j, sA, sB, sStage0, sW, sW1);
+        reconstruct_pair<false>(F.r, j, sA, sB, sStage0, sW);
         __syncthreads();
     }
 }
