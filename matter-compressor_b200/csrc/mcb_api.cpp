@@ -499,29 +499,33 @@ static bool blob_items(const uint8_t *b, uint64_t bl, const uint8_t *d_blob, Dec
     return true;
 }
 
-// Host blobs in, host voxels out, as a two-slot pipeline over groups of
-// kBlobGroup chunks: while one slot's voxels travel device->host, the other
-// slot's blobs travel host->device and decode. A slot is reused once the
-// event recorded after its previous group's copy-out has fired.
+// Host blobs in, host voxels out, as a pipeline of kBlobSlots slots over
+// groups of kBlobGroup chunks: while one slot's voxels travel device->host,
+// the next slots' blobs travel host->device and decode. A slot is reused once
+// the event recorded after its previous group's copy-out has fired; with
+// three slots the host prepares a group while two are still in flight, so a
+// group's decode (about as long as a group's copy-out at 8 chunks) is queued
+// before the link runs dry.
 int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens, int n, mc_u8 *out,
                                size_t out_stride) {
     if (n < 0 || (n && (!blobs || !lens || !out))) return -1;
     Lane *L = lane();
     if (!L) return -1;
     constexpr int kBlobGroup = 8;
-    bool ok = blob_slot_ready(L->pipe[0]) && blob_slot_ready(L->pipe[1]);
+    bool ok = true;
+    for (int k = 0; k < kBlobSlots; ++k) ok = ok && blob_slot_ready(L->pipe[k]);
     uint32_t bad = 0;
-    int used[2] = {0, 0};
+    int used[kBlobSlots] = {};
     auto collect = [&](BlobSlot &S, int &u) {   // after S.done: count its cut-short blocks
         if (u && S.batch.h_status.p) bad += *S.batch.h_status.as<uint32_t>();
         u = 0;
     };
     for (int c0 = 0, gi = 0; ok && c0 < n; c0 += kBlobGroup, ++gi) {
-        BlobSlot &S = L->pipe[gi & 1];
+        BlobSlot &S = L->pipe[gi % kBlobSlots];
         const int g = std::min(kBlobGroup, n - c0);
         ok = cuda_ok(cudaEventSynchronize(S.done), "event sync");
         if (!ok) break;
-        collect(S, used[gi & 1]);
+        collect(S, used[gi % kBlobSlots]);
         uint64_t total = 0;
         uint64_t at[kBlobGroup];
         for (int j = 0; j < g; ++j) {
@@ -555,9 +559,9 @@ int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens
                                              kChunkBytes, cudaMemcpyDeviceToHost, S.stream), "D2H");
         }
         ok = ok && cuda_ok(cudaEventRecord(S.done, S.stream), "event record");
-        used[gi & 1] = 1;
+        used[gi % kBlobSlots] = 1;
     }
-    for (int k = 0; k < 2; ++k) {   // drain both slots, also after an error
+    for (int k = 0; k < kBlobSlots; ++k) {   // drain every slot, also after an error
         if (L->pipe[k].stream && cuda_ok(cudaStreamSynchronize(L->pipe[k].stream), "sync")) collect(L->pipe[k], used[k]);
         else ok = false;
     }

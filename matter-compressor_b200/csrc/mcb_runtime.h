@@ -91,6 +91,9 @@ struct BlobSlot {
     ~BlobSlot();
 };
 // Per-thread execution resources: a stream and reusable buffers.
+// Slots of the host-blob decode pipeline (mc_b200_decode_chunk_blobs).
+constexpr int kBlobSlots = 3;
+
 struct Lane {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -104,7 +107,7 @@ struct Lane {
     DevBuf smp_grid, smp_cand, smp_acc;         // box sampling: block-fraction grid, candidates, accept flags
     HostBuf h_items, h_base, h_stage, h_misc;
     LaunchCfg cfg;
-    BlobSlot pipe[2];
+    BlobSlot pipe[kBlobSlots];
     ~Lane();
 };
 Lane *lane();

@@ -51,13 +51,14 @@ def test_chunk_blobs_decode_golden(gpu, golden_chunks):
 
 
 def test_chunk_blobs_pipeline(gpu, golden_chunks):
-    """More blobs than one pipeline group (three groups over both slots), a
-    missing blob, and a padded output stride: every chunk still matches."""
+    """More blobs than the pipeline has slots (five groups of up to 8 over
+    three slots, so two slots are reused), a missing blob, and a padded output
+    stride: every chunk still matches."""
     import ctypes as C
     g = golden_chunks
     blobs = [g["blobs"][g["offs"][i]:g["offs"][i + 1]] for i in range(len(g["offs"]) - 1)]
     want = [str(s) for s in g["decoded_sha"]]
-    seq = [(i * 5) % len(blobs) for i in range(19)]
+    seq = [(i * 5) % len(blobs) for i in range(35)]
     arrs = [blobs[i] for i in seq]
     ptrs = (C.c_void_p * len(arrs))(*[(a.ctypes.data if a.size else None) for a in arrs])
     lens = np.asarray([a.size for a in arrs], np.uint64)
