@@ -294,7 +294,7 @@ void mc_archive_decode_block(mc_archive *a, uint64_t co, int bz, int by, int bx,
     it.qslot = (uint16_t)slot;
     it.clip_lo = kClipFullLo;
     it.clip_hi = kClipFullHi;
-    if (!decode_items(*L, &it, 1) ||
+    if (!decode_one(*L, it) ||
         !cuda_ok(cudaMemcpyAsync(L->h_stage.p, L->out.p, kN3, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
         !finish(*L, nullptr)) {
         memset(dst, 0, kN3);

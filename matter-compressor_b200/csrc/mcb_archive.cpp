@@ -477,7 +477,7 @@ void mc_dec_block(mc_codec_ctx *C, const mc_u8 *p, uint32_t plen, mc_u8 *dst) {
     it.clip_lo = kClipFullLo;
     it.clip_hi = kClipFullHi;
     if ((plen && !cuda_ok(cudaMemcpyAsync(L->src.p, hs, plen, cudaMemcpyHostToDevice, L->stream), "H2D")) ||
-        !decode_items(*L, &it, 1) ||
+        !decode_one(*L, it) ||
         !cuda_ok(cudaMemcpyAsync(hs, L->out.p, kN3, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
         !cuda_ok(cudaStreamSynchronize(L->stream), "sync")) {
         memset(dst, 0, kN3);

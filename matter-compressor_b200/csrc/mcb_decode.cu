@@ -1072,6 +1072,102 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
     }
 }
 
+// ---------------------------------------------------------------- one block
+// The single-block calls (mc_archive_decode_block, mc_dec_block): one CTA
+// decodes one block end to end in one launch, with the work item as a kernel
+// argument -- no batch layout, no host-to-device copies, no second launch.
+// Thread 0 runs the entropy decode through the k_entropy step functions
+// (fast_step pairs, slow_step for the rare states), the CTA then reconstructs
+// the block. A branchy scalar loop over the same states was measured slower
+// per bin (p99 block latency 1.23 ms against 0.93): each bin's shared-memory
+// context load and branch resolution then sit on the serial chain, which the
+// warp step avoids by fetching both candidate contexts ahead, without
+// branches.
+
+// The whole stream of one block on one lane: the k_entropy loop with one
+// live lane.
+__device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, uint32_t *ctx,
+                                             const uint16_t *s_bend) {
+    while (L.st < S_DONE) {
+        while (L.st <= F_EGP) {
+            fast_step<true>(L, P, ctx, s_bend);    // the lane is live here
+            fast_step<false>(L, P, ctx, s_bend);   // the first step may have left it in a slow state
+        }
+        if (L.st < S_DONE) slow_step(L, P);
+    }
+}
+
+static_assert(sizeof(DecItem) % 16 == 0, "SoloScratch::hdr must sit on a 16-byte boundary");
+
+__global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, const QTab *qtab,
+                                                    const uint16_t *scan, uint32_t *status) {
+    // sA holds thread 0's entropy contexts (one column of 32-word rows, the
+    // layout k_entropy uses) until the entropy decode is done, then the
+    // pass-1 output
+    __shared__ __align__(16) float sA[16 * 16 * kRowF];
+    __shared__ __align__(16) float sB[kBoxB];
+    __shared__ __align__(16) uint8_t sStage[kStageBytes];
+    __shared__ __align__(16) float4 sW[16 * 8];
+    __shared__ uint16_t s_bend[9];
+    static_assert(sizeof(sA) >= sizeof(uint32_t) * kCtxSlots * 32, "contexts fit in sA");
+    const int tid = threadIdx.x;
+    for (int i = tid + 1; i < kN3; i += blockDim.x) {
+        const uint32_t b = scan[i] >> 12;
+        if ((scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
+    }
+    for (int i = tid; i < 16 * 8; i += blockDim.x) {
+        const int k = i >> 3, mm = (i & 7) * 2;
+        sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
+    }
+    rec_init(sB);
+    const uint32_t cap = entry_cap(it.len);
+    if (tid == 0) {
+        s_bend[7] = kN3;
+        s_bend[8] = 0xFFFF;
+        S->item = it;
+        S->base = 0;
+        S->pool_used = 0;
+        status[0] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        EntParams P;
+        P.items = &S->item;
+        P.order = nullptr;
+        P.n = 1;
+        P.ncoded = 1;
+        P.base = &S->base;
+        P.arena = S->entries;
+        P.hdr = &S->hdr;
+        P.pool = S->entries + cap;       // the overflow continues the list
+        P.pool_cap = kEntryMax - cap;    // what one block may ask of the pool
+        P.pool_used = &S->pool_used;
+        P.qtab = qtab;
+        P.scan = scan;
+        P.status = status;
+        P.counter = nullptr;
+        uint32_t *ctx = reinterpret_cast<uint32_t *>(sA);
+        LaneState L;
+        memset(&L, 0, sizeof L);
+        lane_begin(L, P, ctx, s_bend, 0);
+        solo_entropy(L, P, ctx, s_bend);
+        lane_finish(L, P);
+    }
+    __syncthreads();   // thread 0's header and entries are visible to the CTA
+    RecParams R;
+    R.items = &S->item;
+    R.idx = nullptr;
+    R.n = 1;
+    R.hdr = &S->hdr;
+    R.base = &S->base;
+    R.arena = S->entries;
+    R.pool = S->entries + cap;
+    R.qtab = qtab;
+    R.scan = scan;
+    reconstruct_block<true>(R, 0, sA, sB, sStage, sW);   // written in this kernel: read through L2
+    store_block(it, sStage);
+}
+
 // ---------------------------------------------------------------- launchers
 cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s) {
     return cudaMemcpyToSymbolAsync(c_cos, cmf, sizeof(float) * 256, 0, cudaMemcpyHostToDevice, s);
@@ -1141,6 +1237,12 @@ cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStr
         carve_set |= 1ull << (dev & 63);
     }
     k_reconstruct<<<blocks, 128, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_one(const DecItem &it, SoloScratch *scratch, const QTab *qtab, const uint16_t *scan,
+                              uint32_t *status, cudaStream_t s) {
+    k_decode_one<<<1, 128, 0, s>>>(it, scratch, qtab, scan, status);
     return cudaGetLastError();
 }
 

@@ -107,6 +107,21 @@ cudaError_t launch_gather_boxes(const GatherItem *d_items, int nitems, uint32_t 
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStream_t s);
 
+// Device scratch of the single-block decode (k_decode_one): the block's work
+// item, its entropy header and its entry list.
+struct SoloScratch {
+    DecItem item;                  // offset 0 (16-byte aligned buffer)
+    EntHdr hdr;                    // read back as one 16-byte load
+    uint64_t base;                 // the block's entries start the list: 0
+    uint32_t pool_used, pad;
+    uint32_t entries[kEntryMax];   // the first entry_cap(len) are the arena, the rest the overflow pool
+};
+// One block end to end in one CTA: scalar entropy decode on one thread, then
+// the CTA's reconstruction and clipped store. status[0] becomes the number of
+// cut-short blocks (0 or 1).
+cudaError_t launch_decode_one(const DecItem &it, SoloScratch *scratch, const QTab *qtab, const uint16_t *scan,
+                              uint32_t *status, cudaStream_t s);
+
 // ---- encode ----
 // One 16^3 block to encode, gathered from a strided u8 source.
 struct EncItem {

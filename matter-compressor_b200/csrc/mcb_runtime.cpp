@@ -375,6 +375,19 @@ bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s) {
     return cuda_ok(cudaEventRecord(L.done, s), "event record");
 }
 
+bool decode_one(Lane &L, const DecItem &it) {
+    Runtime *R = runtime();
+    if (!R) return false;
+    // the previous batch may still use the lane's status word
+    if (!cuda_ok(cudaEventSynchronize(L.done), "event sync") || !L.solo.ensure(sizeof(SoloScratch)) ||
+        !L.batch.status.ensure(16))
+        return false;
+    return cuda_ok(launch_decode_one(it, L.solo.as<SoloScratch>(), R->d_qtab, R->d_scan, L.batch.status.as<uint32_t>(),
+                                     L.stream),
+                   "single-block decode launch") &&
+           cuda_ok(cudaEventRecord(L.done, L.stream), "event record");
+}
+
 uint32_t lane_bad_blocks(Lane &L) {
     uint32_t v = 0;
     if (L.batch.status.p) cudaMemcpy(&v, L.batch.status.p, 4, cudaMemcpyDeviceToHost);

@@ -105,6 +105,7 @@ struct Lane {
     DevBuf pyr_stage, pyr_a, pyr_b, pyr_flag;   // LOD pyramid: chunk staging, level volumes, all-air flags
     DevBuf ver_items, ver_bad;                  // device verify: blob list, mismatch flags
     DevBuf smp_grid, smp_cand, smp_acc;         // box sampling: block-fraction grid, candidates, accept flags
+    DevBuf solo;                                // single-block decode scratch (SoloScratch)
     HostBuf h_items, h_base, h_stage, h_misc;
     LaunchCfg cfg;
     BlobSlot pipe[kBlobSlots];
@@ -127,6 +128,10 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
 // Decodes n items whose src/dst are device addresses (host-side item array),
 // enqueued on stream s (null: the lane's stream); false on a launch error.
 bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s = nullptr);
+// One block on the lane's stream through the single-block kernel (no
+// batch layout, no copies): the output lands at it.dst; the lane's status
+// word reports whether its stream was cut short.
+bool decode_one(Lane &L, const DecItem &it);
 
 // Encodes chunks of 256^3 voxels resident on the device (chunk c at
 // d_vox[c]) into assembled blobs. Synchronises; on return blob_len[c]
