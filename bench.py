@@ -46,7 +46,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per decoded chunk of the entropy stage, measured
 # with ncu on a 16-chunk case and scaled per chunk
 # (profiles/k_entropy_decode_q6_16chunks.md).
-ENTROPY_DRAM_BYTES_PER_CHUNK = 16.690176e6 / 16
+ENTROPY_DRAM_BYTES_PER_CHUNK = (12.763136e6 + 3.737856e6) / 16
 
 
 def parse():
