@@ -721,6 +721,11 @@ def run_reference(args, d):
 def run_b200(args, d):
     from mcb200 import McLib, decode_chunk_blobs
     lib = McLib.product()
+    # each rank's library runs on the rank's own GPU (its current device, set
+    # before any CUDA work): a rank bound elsewhere would time the wrong GPU
+    if lib.L.mc_b200_device() != torch.cuda.current_device():
+        raise RuntimeError(f"rank {d.rank}: library on device {lib.L.mc_b200_device()}, "
+                           f"torch on device {torch.cuda.current_device()}")
     dev = torch.device("cuda", torch.cuda.current_device())
     seeds = chunk_seeds(d.rank, args.chunks)
     vox = make_volumes(seeds, dev)

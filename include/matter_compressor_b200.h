@@ -132,6 +132,10 @@ int        mc_reader_nlods(mc_reader *r);                                       
 /* Runtime. mc_b200_init returns 0 when an sm_100 device is usable, -1 (with
  * the reason in mc_b200_last_error) otherwise. The last error is per thread. */
 int  mc_b200_init(void);
+/* The CUDA device ordinal the library's runtime is bound to (the calling
+ * thread's current device at the library's first use; one device per
+ * process), or -1 without a usable device. No reference counterpart. */
+int  mc_b200_device(void);
 const char *mc_b200_last_error(void);
 void mc_b200_clear_error(void);
 /* Blocks of the calling thread's last decode whose corrupt stream was cut

@@ -262,6 +262,10 @@ extern "C" {
 
 // ============================================================ runtime
 int mc_b200_init(void) { return runtime() ? 0 : -1; }
+int mc_b200_device(void) {
+    Runtime *R = runtime();
+    return R ? R->device : -1;
+}
 const char *mc_b200_last_error(void) { return last_error(); }
 void mc_b200_clear_error(void) { clear_error(); }
 uint32_t mc_b200_last_bad_blocks(void) {

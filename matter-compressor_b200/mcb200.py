@@ -98,6 +98,7 @@ class McLib:
         if b200:
             sig.update({
                 "mc_b200_init": (i, []),
+                "mc_b200_device": (i, []),
                 "mc_b200_last_error": (C.c_char_p, []),
                 "mc_b200_clear_error": (None, []),
                 "mc_b200_last_bad_blocks": (u32, []),

@@ -33,6 +33,12 @@ def test_block_encode_golden(gpu, golden_blocks):
         assert got == want, f"case {i}: kind {int(g['kind'][i])} q={float(g['q'][i])} tau={int(g['tau'][i])}"
 
 
+def test_runtime_device_is_callers(gpu):
+    """The library's runtime sits on the caller's current device."""
+    import torch
+    assert gpu.L.mc_b200_device() == torch.cuda.current_device()
+
+
 def test_corrupt_streams_golden(gpu, golden_corrupt):
     g = golden_corrupt
     for i in range(len(g["q"])):
