@@ -662,7 +662,15 @@ cudaError_t launch_encode(const EncParams &p, cudaStream_t s) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = p.n < sms * 5 ? p.n : sms * 5;   // 45.6 KB of shared memory: 5 CTAs per SM
+    // one wave of CTAs: as many per SM as fit (45.6 KB of shared memory plus
+    // the per-CTA reserve, in allocation units, leaves room for 4). CTAs walk
+    // the blocks with a fixed stride, so CTAs beyond one wave would start
+    // their whole share late.
+    static int occ_by_dev[64] = {0};
+    int &occ = occ_by_dev[dev & 63];
+    if (occ == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_encode, 128, smem) != cudaSuccess || occ < 1))
+        occ = 1;
+    int blocks = p.n < sms * occ ? p.n : sms * occ;
     k_encode<<<blocks, 128, smem, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
