@@ -18,7 +18,12 @@ C API and records inputs, payload bytes and digests of decoded outputs:
   deblock.npz  digests of mc_deblock's output on the shapes.deblock_volumes()
                inputs over a set of qualities (the volume is followed by a
                zero plane, so the reference's read past the last z face sees
-               zeros).
+               zeros);
+  priors.npz   per-volume trained priors (shapes.priors_tables()): block
+               encode/decode vectors under mc_codec_set_priors, and an archive
+               whose prior blob is stamped by mc_archive_set_priors before the
+               shapes.priors_sequence() appends -- its file digest and every
+               chunk's decoded digest.
 
 Inputs are deterministic integer formulas (shapes.py) so tests regenerate
 them exactly. Usage: python tests/golden/make_golden.py
@@ -159,6 +164,7 @@ def main():
     print("chunks:", len(blobs), "blobs,", int(boffs[-1]), "bytes; archive", len(data), "bytes")
     deblock_golden(ref)
     pyramid_golden(ref)
+    priors_golden(ref)
 
 
 PYRAMID_QS = [6.0, 0.25]
@@ -229,10 +235,54 @@ def deblock_golden(ref):
     print("deblock:", len(digests), "cases")
 
 
+PRIORS_QS = [1.0, 3.0, 6.0, 12.0]
+PRIORS_TAUS = [0, 4]
+
+
+def priors_golden(ref):
+    plo, phi = shapes.priors_tables()
+    kinds, qs, taus, pays, dsha = [], [], [], [], []
+    ref.set_priors(plo, phi)
+    try:
+        for k, vox in enumerate(shapes.block_patterns()):
+            for q in PRIORS_QS:
+                for tau in PRIORS_TAUS:
+                    p = ref.enc_block(vox, q, tau)
+                    kinds.append(k)
+                    qs.append(q)
+                    taus.append(tau)
+                    pays.append(np.frombuffer(p, np.uint8))
+                    dsha.append(sha(ref.dec_block(p, q)))
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "priors.mca")
+            names, csha = [], []
+            with ref.open(path, 512, 256, 256, 6.0) as a:
+                assert ref.L.mc_archive_set_priors(a.a, plo.ctypes.data, phi.ctypes.data) == 0
+                for step in shapes.priors_sequence():
+                    vox = shapes.chunk_source(step["src"])
+                    if step["op"] == "par":
+                        rc = a.append_par(0, *step["at"], vox, step["q"])
+                    else:
+                        rc = a.append_ctx(0, *step["at"], vox, 8.0, preset=step["preset"])
+                    assert rc == 0, step
+                    names.append(step["name"])
+                    csha.append(sha(a.decode_chunk(a.chunk_offset(0, *step["at"]))))
+            data = open(path, "rb").read()
+    finally:
+        ref.set_priors(None, None)
+    offs = np.cumsum([0] + [len(p) for p in pays]).astype(np.int64)
+    np.savez_compressed(os.path.join(HERE, "priors.npz"), plo=plo, phi=phi, kind=np.array(kinds, np.int32),
+                        q=np.array(qs, np.float32), tau=np.array(taus, np.int32), offs=offs,
+                        payload=np.concatenate(pays), decoded_sha=np.array(dsha), chunk_names=np.array(names),
+                        chunk_sha=np.array(csha), archive_sha=np.array(hashlib.sha256(data).hexdigest()),
+                        archive_len=np.array(len(data), np.int64))
+    print("priors:", len(pays), "blocks,", len(names), "chunks; archive", len(data), "bytes")
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] in (["deblock"], ["pyramid"]):
+    if sys.argv[1:] in (["deblock"], ["pyramid"], ["priors"]):
         r = McLib(REF, b200=False)
         r.L.mc_codec_init()
-        (deblock_golden if sys.argv[1] == "deblock" else pyramid_golden)(r)
+        {"deblock": deblock_golden, "pyramid": pyramid_golden, "priors": priors_golden}[sys.argv[1]](r)
     else:
         main()

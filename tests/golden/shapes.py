@@ -173,3 +173,25 @@ def blob_len(data, co):
     npres = int(np.unpackbits(bm).sum())
     lens = np.frombuffer(data, np.uint16, npres, co + 14 + fml + 512)
     return 14 + fml + 512 + 2 * npres + int(lens.astype(np.int64).sum())
+
+
+def priors_tables():
+    """A per-volume prior pair (q=1 and q=12 endpoint tables, u16[8][32]) that
+    differs from the baked corpus tables in every trained slot, as a volume's
+    own training would: probabilities stay inside the coder's usable range
+    [48, 4048]. Deterministic integer formula."""
+    c, s = np.meshgrid(np.arange(8), np.arange(32), indexing="ij")
+    plo = 48 + (c * 613 + s * 389 + 97) % 4001
+    phi = 48 + (c * 271 + s * 757 + 1301) % 4001
+    return plo.astype(np.uint16), phi.astype(np.uint16)
+
+
+def priors_sequence():
+    """Appends into a 512x256x256 archive that carries the priors_tables()
+    blob: a parallel append at q=6, a preset-ladder append (max error) and a
+    parallel append at q=1."""
+    return [
+        {"name": "waves_par_q6", "op": "par", "at": (0, 0, 0), "q": 6.0, "src": "waves"},
+        {"name": "tex_preset3", "op": "ctx", "at": (0, 0, 1), "preset": 3, "src": "sphere_tex"},
+        {"name": "half_par_q1", "op": "par", "at": (1, 0, 0), "q": 1.0, "src": "half_air"},
+    ]

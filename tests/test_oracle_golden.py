@@ -108,3 +108,45 @@ def test_pyramid(oracle):
         for key, c in chunks.items():
             blob = oracle.encode_chunk(c.reshape(-1), q, 0, header_q=q)
             assert hashlib.sha256(blob).hexdigest() == want[key], (q, key)
+
+
+PRESETS = [(0.5, 1), (0.5, 2), (1.0, 4), (2.5, 8), (6.0, 16), (16.0, 32), (32.0, 64), (64.0, 128)]
+
+
+@pytest.fixture
+def golden_priors(oracle):
+    g = np.load(os.path.join(GOLDEN, "priors.npz"))
+    oracle.set_priors(g["plo"], g["phi"])
+    yield g
+    oracle.set_priors(None, None)
+
+
+def test_priors_blocks(oracle, golden_priors):
+    """Per-volume priors (src/mc_codec.c:144-167): block payloads and decoded
+    blocks under a non-default prior pair match the reference's."""
+    g = golden_priors
+    pats = shapes.block_patterns()
+    differ = 0
+    for i in range(len(g["q"])):
+        q, tau, k = float(g["q"][i]), int(g["tau"][i]), int(g["kind"][i])
+        want = g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()
+        got = oracle.enc_block(pats[k], q, tau)
+        assert got == want, f"case {i}: pattern {k} q={q} tau={tau}"
+        dec = oracle.dec_block(got, q) if got else np.zeros(4096, np.uint8)
+        assert sha(dec) == g["decoded_sha"][i], f"case {i} decode"
+        oracle.set_priors(None, None)
+        differ += oracle.enc_block(pats[k], q, tau) != want
+        oracle.set_priors(g["plo"], g["phi"])
+    assert differ > len(g["q"]) // 2   # the prior pair really changes the bit stream
+
+
+def test_priors_chunks(oracle, golden_priors):
+    """Chunks appended to an archive whose priors were stamped by
+    mc_archive_set_priors (src/mc_archive.c:650-662) decode to the reference's
+    voxels when the oracle codes them under the same priors."""
+    g = golden_priors
+    for i, st in enumerate(shapes.priors_sequence()):
+        vox = shapes.chunk_source(st["src"])
+        q, tau = (st["q"], 0) if st["op"] == "par" else PRESETS[st["preset"]]
+        blob = oracle.encode_chunk(vox, q, tau)
+        assert sha(oracle.decode_chunk(blob)) == g["chunk_sha"][i], st["name"]
