@@ -307,9 +307,12 @@ void mc_b200_server_close(mc_b200_server *s);
  * stream); the call returns before it ends.
  *
  * Limits: n <= 4096, and the sum over blocks of min(12288, 8*len_i + 64)
- * <= 4194304 (about 512 KiB of payload); larger requests return -2 / -3 and
- * must be split. d_payloads must be 8-byte aligned with 16 readable bytes
- * after the last payload. Corrupt payloads decode as the reference decodes
+ * <= 4194304 (the per-block coefficient bound; a block of 1500 bytes or more
+ * counts 12288); larger requests return -2 / -3 and must be split. d_payloads
+ * must be 8-byte aligned with 16 readable bytes after the last payload;
+ * d_out must hold n*4096 bytes. The payload lengths and the quality table
+ * travel to the GPU inside the kernel launch itself, so the call keeps no
+ * host buffer once it returns. Corrupt payloads decode as the reference decodes
  * them, except that their spill past the fixed 1 MiB overflow area is cut
  * short; no bad-block count is kept.
  * Returns 0, or -1 (bad arguments), -2, -3 (limits), -4 (CUDA error); each

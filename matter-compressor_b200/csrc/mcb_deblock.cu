@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mcb_devinfo.h"
 #include "mcb_kernels.h"
 
 namespace mcb {
@@ -129,12 +130,7 @@ __global__ void __launch_bounds__(256) k_deblock_z16(DbParams P) {
     }
 }
 
-static int db_sms() {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms;
-}
+static int db_sms() { return dev_sms(); }
 
 static uint32_t faces(uint32_t n) { return n > 16 ? (n - 1) / 16 : 0; }
 

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mcb_devinfo.h"
 #include "mcb_format.h"
 #include "mcb_kernels.h"
 
@@ -1173,16 +1174,7 @@ cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s) {
     return cudaMemcpyToSymbolAsync(c_cos, cmf, sizeof(float) * 256, 0, cudaMemcpyHostToDevice, s);
 }
 
-static int g_num_sms = 0;
-static int num_sms() {
-    if (!g_num_sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_num_sms <= 0) g_num_sms = 148;
-    }
-    return g_num_sms;
-}
+static int num_sms() { return dev_sms(); }
 
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s) {
     if (p.ncoded <= 0) return cudaSuccess;
@@ -1195,18 +1187,17 @@ cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_
 }
 
 int fused_grid(const LaunchCfg &cfg) {
-    static int occ_by_dev[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int &occ = occ_by_dev[dev & 63];
-    if (occ == 0) {
+    static std::atomic<int> occ_by_dev[kMaxDevs];
+    const int occ = dev_once(occ_by_dev, [] {
         // dynamic shared memory above 48 KiB: opt in once per device
+        int o = 0;
         if (cudaFuncSetAttribute(k_decode_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(FusedSmem)) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_decode_fused, 128, sizeof(FusedSmem)) !=
-                cudaSuccess || occ < 1)
-            occ = -1;
-    }
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_decode_fused, 128, sizeof(FusedSmem)) !=
+                cudaSuccess || o < 1)
+            o = -1;
+        return o;
+    });
     if (occ < 0) return 0;
     // every CTA resident at once: a CTA's waits are then on CTAs that run
     const int per_sm = std::min(cfg.fused_ctas_per_sm > 0 ? cfg.fused_ctas_per_sm : 4, occ);
@@ -1228,14 +1219,13 @@ cudaError_t launch_reconstruct(const RecParams &p, const LaunchCfg &cfg, cudaStr
     int blocks = (p.n + 1) / 2;   // one CTA step per pair of blocks
     int cap = num_sms() * (cfg.rec_ctas_per_sm > 0 ? cfg.rec_ctas_per_sm : 5);
     if (blocks > cap) blocks = cap;
-    static unsigned long long carve_set = 0;   // per device: the largest shared-memory carveout, 5 CTAs/SM fit
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(carve_set >> (dev & 63) & 1ull)) {
+    // per device: the largest shared-memory carveout, so that 5 CTAs per SM fit
+    static std::atomic<int> carve_set[kMaxDevs];
+    dev_once(carve_set, [] {
         cudaFuncSetAttribute(k_reconstruct, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
-        carve_set |= 1ull << (dev & 63);
-    }
+        return 1;
+    });
     k_reconstruct<<<blocks, 128, 0, s>>>(p);
     return cudaGetLastError();
 }

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mcb_devinfo.h"
 #include "mcb_format.h"
 #include "mcb_kernels.h"
 
@@ -649,27 +650,29 @@ cudaError_t upload_cos_encode(const float cmf[16][16], cudaStream_t s) {
 
 cudaError_t launch_encode(const EncParams &p, cudaStream_t s) {
     if (p.n <= 0) return cudaSuccess;
-    static bool attr = false;
     const int smem = (int)sizeof(EncSmem);
-    if (!attr) {
+    // per device: the dynamic shared memory opt-in and the carveout (1), or
+    // the error code of the attribute call that failed (negated)
+    static std::atomic<int> attr[kMaxDevs];
+    const int a = dev_once(attr, [smem] {
         cudaError_t e = cudaFuncSetAttribute(k_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k_encode, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_encode, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        return e == cudaSuccess ? 1 : -(int)e;
+    });
+    if (a < 0) return (cudaError_t)(-a);
+    const int sms = dev_sms();
     // one wave of CTAs: as many per SM as fit (45.6 KB of shared memory plus
     // the per-CTA reserve, in allocation units, leaves room for 4). CTAs walk
     // the blocks with a fixed stride, so CTAs beyond one wave would start
     // their whole share late.
-    static int occ_by_dev[64] = {0};
-    int &occ = occ_by_dev[dev & 63];
-    if (occ == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_encode, 128, smem) != cudaSuccess || occ < 1))
-        occ = 1;
+    static std::atomic<int> occ_by_dev[kMaxDevs];
+    const int occ = dev_once(occ_by_dev, [smem] {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_encode, 128, smem) != cudaSuccess || o < 1) o = 1;
+        return o;
+    });
     int blocks = p.n < sms * occ ? p.n : sms * occ;
     k_encode<<<blocks, 128, smem, s>>>(p);
     cudaError_t e = cudaGetLastError();

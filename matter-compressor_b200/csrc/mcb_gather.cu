@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mcb_devinfo.h"
 #include "mcb_format.h"
 #include "mcb_kernels.h"
 
@@ -65,12 +66,7 @@ __global__ void __launch_bounds__(128) k_gather_boxes(const GatherItem *items, i
     }
 }
 
-static int sm_count() {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms;
-}
+static int sm_count() { return dev_sms(); }
 
 cudaError_t launch_table_update(const uint2 *d_upd, int n, uint32_t *d_tables, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;

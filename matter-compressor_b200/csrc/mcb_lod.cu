@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mcb_devinfo.h"
 #include "mcb_kernels.h"
 
 namespace mcb {
@@ -67,12 +68,7 @@ __global__ void __launch_bounds__(256) k_gather_chunk(const uint8_t *__restrict_
     if (__any_sync(0xFFFFFFFFu, nonzero) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
-static int lod_sms() {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms;
-}
+static int lod_sms() { return dev_sms(); }
 
 cudaError_t launch_decimate(const uint8_t *d_src, int dz, int dy, int dx, uint8_t *d_dst, cudaStream_t s) {
     if (dz <= 0 || dy <= 0 || dx <= 0) return cudaErrorInvalidValue;

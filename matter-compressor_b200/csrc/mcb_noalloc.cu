@@ -31,8 +31,7 @@ constexpr uint32_t kNaPoolEntries = 256u << 10;     // overflow pool for corrupt
 
 // Scratch layout (byte offsets, each 256-aligned).
 constexpr size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
-constexpr size_t kOffOffsets = 0;
-constexpr size_t kOffItems = align256(kOffOffsets + 8 * (kNaMaxBlocks + 1));
+constexpr size_t kOffItems = 0;
 constexpr size_t kOffBase = align256(kOffItems + sizeof(DecItem) * kNaMaxBlocks);
 constexpr size_t kOffHdr = align256(kOffBase + 8 * kNaMaxBlocks);
 constexpr size_t kOffScan = align256(kOffHdr + sizeof(EntHdr) * kNaMaxBlocks);
@@ -55,66 +54,85 @@ struct DevSetup {
 constexpr int kMaxDevices = 64;
 DevSetup g_setup[kMaxDevices];
 std::mutex g_mu;
-// Host staging for the per-call uploads (static: no allocation).
-uint64_t g_offsets[kNaMaxBlocks + 1];
-QTab g_qtab;
 
-// One CTA of 1024 threads: builds the work list from the payload offsets,
-// the arena offsets (exclusive prefix sum of each block's entry bound) and
-// clears the status words.
-__global__ void __launch_bounds__(1024) k_noalloc_prepare(uint8_t *scratch, const uint8_t *payloads, int n,
+// What a call passes to the GPU: the payload lengths and the quality table
+// travel by value as the kernel's parameter (copied at launch), so no host
+// buffer outlives the call and concurrent calls from several host threads
+// share nothing on the host. 16.8 KB, within the 32,764-byte parameter limit.
+struct NaCall {
+    QTab qtab;
+    uint64_t start;                 // h_offsets[0]
+    int n;
+    uint32_t len[kNaMaxBlocks];     // payload bytes of block i
+};
+static_assert(sizeof(NaCall) < 32764, "kernel parameter size limit");
+
+// One CTA of 1024 threads: writes the quality table into the scratch, builds
+// the work list from the payload lengths (payload offsets and arena offsets
+// are exclusive prefix sums over the blocks, the latter of each block's entry
+// bound) and clears the status words.
+__global__ void __launch_bounds__(1024) k_noalloc_prepare(const NaCall c, uint8_t *scratch, const uint8_t *payloads,
                                                           uint8_t *out) {
-    const uint64_t *off = reinterpret_cast<const uint64_t *>(scratch + kOffOffsets);
     DecItem *items = reinterpret_cast<DecItem *>(scratch + kOffItems);
     uint64_t *base = reinterpret_cast<uint64_t *>(scratch + kOffBase);
     uint32_t *status = reinterpret_cast<uint32_t *>(scratch + kOffStatus);
-    __shared__ uint32_t s_warp[32];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    __shared__ uint64_t s_warp[32][2];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, n = c.n;
     if (tid < 4) status[tid] = 0;   // bad blocks, pool use, work counter
-    uint32_t cap[4], sum = 0;
+    {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(&c.qtab);
+        uint32_t *d = reinterpret_cast<uint32_t *>(scratch + kOffQtab);
+        for (int i = tid; i < (int)(sizeof(QTab) / 4); i += blockDim.x) d[i] = q[i];
+    }
+    uint32_t cap[4];
+    uint64_t csum = 0, lsum = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int i = tid * 4 + j;
-        cap[j] = 0;
+        const uint32_t len = i < n ? c.len[i] : 0u;
+        cap[j] = i < n ? entry_cap(len) : 0u;
+        csum += cap[j];
+        lsum += len;
+    }
+    // inclusive scans of (entry bound, payload bytes) over the threads
+    uint64_t ic = csum, il = lsum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t vc = __shfl_up_sync(0xFFFFFFFFu, ic, o), vl = __shfl_up_sync(0xFFFFFFFFu, il, o);
+        if (lane >= o) { ic += vc; il += vl; }
+    }
+    if (lane == 31) { s_warp[w][0] = ic; s_warp[w][1] = il; }
+    __syncthreads();
+    if (w == 0) {
+        uint64_t vc = s_warp[lane][0], vl = s_warp[lane][1];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t tc = __shfl_up_sync(0xFFFFFFFFu, vc, o), tl = __shfl_up_sync(0xFFFFFFFFu, vl, o);
+            if (lane >= o) { vc += tc; vl += tl; }
+        }
+        s_warp[lane][0] = vc;
+        s_warp[lane][1] = vl;
+    }
+    __syncthreads();
+    uint64_t acc = ic - csum + (w ? s_warp[w - 1][0] : 0);
+    uint64_t pos = c.start + il - lsum + (w ? s_warp[w - 1][1] : 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int i = tid * 4 + j;
         if (i < n) {
-            const uint32_t len = (uint32_t)(off[i + 1] - off[i]);
             DecItem it;
-            it.src = (uint64_t)(uintptr_t)(payloads + off[i]);
+            it.src = (uint64_t)(uintptr_t)(payloads + pos);
             it.dst = (uint64_t)(uintptr_t)(out + (size_t)i * kN3);
             it.sz = 256;
             it.sy = 16;
-            it.len = len;
+            it.len = c.len[i];
             it.qslot = 0;
             it.clip_lo = kClipFullLo;
             it.clip_hi = kClipFullHi;
             it.pad0 = 0;
             it.pad1 = 0;
             items[i] = it;
-            cap[j] = entry_cap(len);
+            base[i] = acc;
+            pos += c.len[i];
         }
-        sum += cap[j];
-    }
-    uint32_t incl = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) s_warp[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t v = s_warp[lane];
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
-            if (lane >= o) v += t;
-        }
-        s_warp[lane] = v;
-    }
-    __syncthreads();
-    uint64_t acc = incl - sum + (w ? s_warp[w - 1] : 0);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int i = tid * 4 + j;
-        if (i < n) base[i] = acc;
         acc += cap[j];
     }
 }
@@ -122,6 +140,31 @@ __global__ void __launch_bounds__(1024) k_noalloc_prepare(uint8_t *scratch, cons
 int fail(int code, const char *msg) {
     fprintf(stderr, "mc_b200_decode_blocks_noalloc: %s\n", msg);
     return code;
+}
+
+// The scratch's device address on device `dev` (current), set up on the
+// first call there: the address lookup (the array's name is only a host-side
+// stand-in) and the constant tables, synchronously. 0 or -4.
+int device_scratch(int dev, uint8_t **out) {
+    std::lock_guard<std::mutex> g(g_mu);
+    DevSetup &ds = g_setup[dev];
+    if (!ds.ready) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
+        static uint16_t scan[kN3];
+        static float cosm[16][16];
+        table_scan(scan);
+        table_cos(cosm);
+        e = cudaMemcpy(static_cast<uint8_t *>(p) + kOffScan, scan, sizeof scan, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = upload_cos(cosm, nullptr);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
+        if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
+        ds.scratch = static_cast<uint8_t *>(p);
+        ds.ready = true;
+    }
+    *out = ds.scratch;
+    return 0;
 }
 
 }  // namespace
@@ -147,35 +190,15 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return fail(-4, "no current CUDA device");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    std::lock_guard<std::mutex> g(g_mu);
-    DevSetup &ds = g_setup[dev];
-    if (!ds.ready) {
-        // once per device, with that device current: the scratch's device
-        // address (the array's name is only a host-side stand-in) and the
-        // constant tables
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
-        static uint16_t scan[kN3];
-        static float cosm[16][16];
-        table_scan(scan);
-        table_cos(cosm);
-        e = cudaMemcpy(static_cast<uint8_t *>(p) + kOffScan, scan, sizeof scan, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = upload_cos(cosm, nullptr);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
-        if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
-        ds.scratch = static_cast<uint8_t *>(p);
-        ds.ready = true;
-    }
-    uint8_t *sc = ds.scratch;
-    memcpy(g_offsets, h_offsets, sizeof(uint64_t) * (size_t)(n + 1));
-    table_qtab(sanitize_q(quality), &g_qtab);
-    // pageable sources: both copies complete before cudaMemcpyAsync returns
-    cudaError_t e = cudaMemcpyAsync(sc + kOffOffsets, g_offsets, sizeof(uint64_t) * (size_t)(n + 1),
-                                    cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sc + kOffQtab, &g_qtab, sizeof g_qtab, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
-    k_noalloc_prepare<<<1, 1024, 0, s>>>(sc, d_payloads, n, d_out);
+    uint8_t *sc = nullptr;
+    const int rc = device_scratch(dev, &sc);
+    if (rc) return rc;
+    NaCall c;   // on the host stack; the launch copies it
+    table_qtab(sanitize_q(quality), &c.qtab);
+    c.start = h_offsets[0];
+    c.n = n;
+    for (int i = 0; i < n; ++i) c.len[i] = (uint32_t)(h_offsets[i + 1] - h_offsets[i]);
+    k_noalloc_prepare<<<1, 1024, 0, s>>>(c, sc, d_payloads, d_out);
     EntParams ep;
     ep.items = reinterpret_cast<const DecItem *>(sc + kOffItems);
     ep.order = nullptr;
@@ -202,7 +225,7 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     rp.qtab = ep.qtab;
     rp.scan = ep.scan;
     LaunchCfg cfg;
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = launch_entropy(ep, cfg, s);
     if (e == cudaSuccess) e = launch_reconstruct(rp, cfg, s);
     if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));

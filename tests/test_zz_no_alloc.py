@@ -4,8 +4,14 @@ mc_dec_block) and the reference's golden digests.
 
 This file sorts last so that it runs both in a fresh process (alone: the
 first GPU call of the library is the no-alloc one, whose first call sets up
-its tables itself) and after every other GPU test (runtime already up).
+its tables itself) and after every other GPU test (runtime already up). The
+cold first call is also checked in a child process of its own, where nothing
+else has touched the library before it.
 """
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -183,3 +189,86 @@ def test_limits_rejected():
     bad = np.array([0, 10, 5], np.uint64)
     assert L.mc_b200_decode_blocks_noalloc(fake, bad.ctypes.data, 2, 6.0, fake, None) == -1
     assert L.mc_b200_decode_blocks_noalloc(None, offs.ctypes.data, 1, 6.0, fake, None) == -1
+
+
+@pytest.mark.gpu
+def test_empty_payloads_decode_to_zeros(raw_lib, golden_blocks):
+    """Empty payloads (absent blocks) between real ones decode to zeros, as
+    mc_dec_block does with plen = 0 (src/mc_codec.c:739-759), and leave their
+    neighbours intact; two calls in a row."""
+    import torch
+    from mcb200 import McLib
+    g = golden_blocks
+    real = [(i, g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes()) for i in range(len(g["q"]))
+            if float(g["q"][i]) == 6.0 and g["offs"][i + 1] > g["offs"][i]][:24]
+    pays = []
+    for k, (i, p) in enumerate(real):
+        pays.append(b"")
+        pays.append(p)
+        if k % 3 == 0:
+            pays.append(b"")
+    lib = McLib.product()
+    assert not lib.dec_block(b"", 6.0).any()
+    stream = torch.cuda.Stream()
+    runs = []
+    for _ in range(2):
+        na = NoAlloc(raw_lib, pays, stream)
+        assert na.launch(6.0) == 0
+        runs.append(na)
+    stream.synchronize()
+    for na in runs:
+        res = na.result()
+        for k, p in enumerate(pays):
+            want = lib.dec_block(p, 6.0) if p else np.zeros(4096, np.uint8)
+            assert np.array_equal(res[k], want), k
+
+
+def test_empty_payload_reference(ref):
+    """The reference's own mc_dec_block on an empty payload: zeros (the
+    behaviour the no-alloc call's empty payloads reproduce)."""
+    assert not ref.dec_block(b"", 6.0).any()
+    assert not ref.dec_block(b"", 1.0).any()
+
+
+_COLD = r"""
+import sys, hashlib
+import numpy as np
+import torch
+sys.path[:0] = [{pkg!r}, {golden!r}]
+from mcb200 import LIB_PATH, McLib
+g = np.load({blocks!r})
+lib = McLib(LIB_PATH)            # no mc_b200_init: the no-alloc call comes first
+pays, want = [], []
+for i in range(len(g["q"])):
+    if float(g["q"][i]) == 6.0 and g["offs"][i + 1] > g["offs"][i]:
+        pays.append(g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes())
+        want.append(str(g["decoded_sha"][i]))
+offs = np.zeros(len(pays) + 1, np.uint64)
+offs[1:] = np.cumsum([len(p) for p in pays])
+host = np.zeros(int(offs[-1]) + 16, np.uint8)
+for p, o in zip(pays, offs[:-1]):
+    host[int(o):int(o) + len(p)] = np.frombuffer(p, np.uint8)
+d_pay = torch.from_numpy(host).cuda()
+for call in range(2):
+    d_out = torch.full((len(pays) * 4096,), 0xCD, dtype=torch.uint8, device="cuda")
+    rc = lib.L.mc_b200_decode_blocks_noalloc(d_pay.data_ptr(), offs.ctypes.data, len(pays), 6.0, d_out.data_ptr(), None)
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    res = d_out.cpu().numpy().reshape(-1, 4096)
+    for k in range(len(pays)):
+        assert hashlib.sha256(res[k].tobytes()).hexdigest() == want[k], (call, k)
+print("cold no-alloc OK", len(pays))
+"""
+
+
+@pytest.mark.gpu
+def test_cold_first_call_in_fresh_process(golden_blocks):
+    """In a child process whose first library call is the no-alloc one (its
+    one-time set-up: the scratch's address and the tables), two calls give
+    the reference's golden digests."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _COLD.format(pkg=os.path.join(root, "matter-compressor_b200"), golden=os.path.join(root, "tests", "golden"),
+                        blocks=os.path.join(root, "tests", "golden", "blocks.npz"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "cold no-alloc OK" in r.stdout
