@@ -196,6 +196,13 @@ int mc_b200_deblock_dev(mc_u8 *d_vol, int count, size_t vol_stride, int nz, int 
 /* Replace the autotuner's choice (same layout as mc_b200_plan_config) and
  * recapture the plan. 0 on success, -1 on bad arguments or a CUDA error. */
 int  mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]);
+/* Fused layout only: how many times (each a sleep of at most 1 us) a CTA
+ * polls a completion-list position that no block pair has filled yet before
+ * it hands the position to the tail kernel and leaves (default 32768). Any
+ * value gives the same voxels; 0 makes every such wait give up at once, which
+ * moves the waiting pairs to the tail kernel. Recaptures the plan. 0 on
+ * success, -1 on a CUDA error. */
+int  mc_b200_plan_set_fused_wait(mc_b200_plan *p, uint32_t polls);
 void mc_b200_plan_free(mc_b200_plan *p);
 
 /* Batched append: encode n chunks (chunk i's 256^3 voxels at HOST vox[i], or

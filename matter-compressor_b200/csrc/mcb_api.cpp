@@ -655,6 +655,12 @@ int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
     return plan_capture(p) ? 0 : -1;
 }
 
+int mc_b200_plan_set_fused_wait(mc_b200_plan *p, uint32_t polls) {
+    if (!p) return -1;
+    p->cfg.fused_wait_polls = polls;
+    return plan_capture(p) ? 0 : -1;
+}
+
 // ============================================================ device verify
 long mc_b200_verify_archive_dev(const uint8_t *arc, const uint8_t *d_arc, size_t len, int verbose) {
     if (!arc || !d_arc) {

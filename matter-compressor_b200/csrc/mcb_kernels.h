@@ -14,6 +14,9 @@ struct LaunchCfg {
     bool split = false;        // long blocks on a second stream (batches large enough to split)
     bool fused = false;        // both stages in one persistent kernel (k_decode_fused)
     int fused_ctas_per_sm = 4;
+    // fused layout: polls (of at most 1 us each) of an unwritten completion-list
+    // position before a CTA gives the position to k_fused_tail and leaves
+    uint32_t fused_wait_polls = 1u << 15;
 };
 
 struct EntParams {

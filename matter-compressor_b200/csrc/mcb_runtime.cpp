@@ -331,7 +331,7 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
             fp.ws = B.fws.as<uint32_t>();
             fp.pair_cnt = fp.ws + kFusedSkip0 + kFusedMaxSkip;
             fp.rlist = fp.pair_cnt + (m + 1) / 2;
-            fp.spin_limit = 1u << 15;   // polls of at most 1 us each
+            fp.spin_limit = cfg.fused_wait_polls;
             if (!cuda_ok(cudaMemsetAsync(fp.ws, 0, sizeof(uint32_t) * fused_ws_words(m), s), "memset") ||
                 !cuda_ok(launch_fused(fp, cfg, s), "fused decode launch"))
                 return false;

@@ -113,6 +113,7 @@ class McLib:
                 "mc_b200_plan_free": (None, [vp]),
                 "mc_b200_plan_config": (None, [vp, vp]),
                 "mc_b200_plan_set_config": (i, [vp, vp]),
+                "mc_b200_plan_set_fused_wait": (i, [vp, u32]),
                 "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
                 "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
                 "mc_b200_verify_archive_dev": (lg, [vp, vp, sz, i]),
@@ -412,6 +413,12 @@ class Plan:
         """Override the autotuned launch shape and recapture the plan."""
         cfg = np.array([entropy_ctas_per_sm, reconstruct_ctas_per_sm, self.STAGES.index(stages)], np.int32)
         rc = self.lib.L.mc_b200_plan_set_config(self.p, _ptr(cfg))
+        self.lib.check()
+        return rc
+
+    def set_fused_wait(self, polls):
+        """Polls before a fused-layout CTA hands an unfilled list position to the tail kernel."""
+        rc = self.lib.L.mc_b200_plan_set_fused_wait(self.p, polls)
         self.lib.check()
         return rc
 

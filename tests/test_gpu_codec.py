@@ -246,3 +246,34 @@ def test_preset_ladder_tau_bound(gpu, tmp_path):
             dec = a.decode_chunk(a.chunk_offset(0, lvl, 0, 0)).reshape(vox.shape)
             err = np.abs(dec.astype(int) - vox.astype(int))
             assert err.max() <= tau, (lvl, err.max())
+
+
+def test_fused_layout_gives_up_waiting(gpu, oracle, tmp_path):
+    """The fused layout's bounded wait: with a wait limit of zero polls every
+    CTA that meets an unfilled completion-list position hands it to
+    k_fused_tail at once and leaves, so the tail kernel reconstructs most
+    pairs; the voxels are still the oracle's. Nothing here waits forever or
+    faults: the wait simply ends."""
+    import torch
+    import volumes
+    with gpu.open(str(tmp_path / "w.mca"), 512, 256, 256, 6.0) as a:
+        for c in range(2):
+            v = volumes.region(41 + c, (0, 0, 256 * c), (256, 256, 256), 0.45, device="cuda").cpu().numpy()
+            assert a.append_par(0, 0, 0, c, v, 6.0) == 0
+        offs = [a.chunk_offset(0, 0, 0, c) for c in range(2)]
+        data = np.fromfile(str(tmp_path / "w.mca"), np.uint8).tobytes()
+        want = np.concatenate([oracle.decode_chunk(data[o:o + shapes.blob_len(data, o)]) for o in offs])
+        d_out = torch.empty(2 * CHUNK, dtype=torch.uint8, device="cuda")
+        plan = a.plan_chunks(offs, d_out.data_ptr())
+        try:
+            if plan.set_config(5, 5, "fused") != 0:
+                pytest.skip("the fused kernel cannot launch on this device")
+            for polls in (0, 1, 1 << 15):
+                assert plan.set_fused_wait(polls) == 0
+                d_out.fill_(0xEE)
+                for _ in range(2):
+                    plan.launch()
+                torch.cuda.synchronize()
+                assert np.array_equal(d_out.cpu().numpy(), want), polls
+        finally:
+            plan.free()
