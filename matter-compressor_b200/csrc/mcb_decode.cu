@@ -34,26 +34,28 @@ namespace mcb {
 __constant__ float c_cos[16][16];
 
 // ---------------------------------------------------------------- stage 1
-// Lane states. F_SIG, F_MAG, F_SIGN and F_EGP cover nearly every bin of a
-// block and share one branch-light step; the rest are entered a few times per
-// block. The block header (flags, dc, EOB) is decoded when a lane starts its
-// block.
+// Lane states. The three fast states cover every bin of the coefficient loop
+// and share one branch-free step that every lane of a warp runs together; the
+// slow states occur a few times per block and are worked off by the lanes
+// that hold them while the rest of the warp waits (see run_lanes). S_IDLE is
+// a parked lane, a fixed point of the fast step (see park). The block header
+// and EOB are decoded when a lane starts its block.
 enum : uint32_t {
     F_SIG = 0,   // significance of scan position p: context sigb + min(popcount(last 16 flags), 3)
     F_MAG,       // unary magnitude rung k: context 56 + k
-    F_SIGN,      // sign (bypass) of the coefficient at p, magnitude m
-    F_EGP,       // Exp-Golomb prefix (bypass): k counts 12 + the one-bits so far
-    S_EGS,       // Exp-Golomb suffix (bypass, rem bits, 16 at a time)
-    S_CSIGN,     // correction sign (bypass)
-    S_END,       // scan done: corrections or finished
-    S_DONE,
-    S_IDLE
+    F_BYP,       // a bypass bin: the sign of the coefficient at p (m != 0), an Exp-Golomb prefix
+                 // bit (m == 0, rem == 0; k counts 12 + the one-bits) or a suffix bit (rem != 0)
+    S_IDLE,      // no more blocks for this lane
+    S_END,       // scan done: corrections, then the block is finished
+    S_EGS,       // an Exp-Golomb suffix of more than 16 bits (only corrupt streams)
+    S_DONE
 };
-enum : uint32_t { R_MAG = 0, R_CCOUNT, R_CGAP, R_CMAG };
 // Context slots per lane: the 68 adaptive contexts plus one scratch slot that
-// bypass bins read and write in place of a real context.
+// bypass bins read and write in place of a real context. The scratch slot
+// directly follows the magnitude ladder, so "the next rung" of rung 11 is it.
 constexpr int kCtxSlots = kNumCtx + 1;
-constexpr uint32_t kSignSlot = kNumCtx;
+constexpr uint32_t kScr = kNumCtx;
+static_assert(kScr == kCtxMag + 12, "scratch slot follows the 12 magnitude rungs");
 // Exp-Golomb prefixes count in k from this base (the magnitude ladder hands
 // over at its 12th rung with k = 12).
 constexpr uint32_t kEgBase = 12;
@@ -68,12 +70,11 @@ struct LaneState {
     uint32_t w, nxt, sel, jn;  // window word, next word (raw), byte selector, index of the next word
     uint32_t nmask;            // the next word's payload bytes (applied when it enters the window)
     uint32_t code, range;
-    uint32_t st, p, eob, hist, sigb, band, bend, stop, k, m;   // hist: significance flags, newest in bit 0
-    uint32_t cc, pc;           // context slot of the next bin and its probability (coefficient loop)
+    uint32_t st, p, eob, hist, sigb, band, bend, stop;   // hist: significance flags, newest in bit 0
+    uint32_t k, m, rem, acc;   // rung / prefix count, magnitude of the pending sign, suffix bits left and read
+    uint32_t cc, pc;           // context slot of the next bin and its probability
     uint32_t hdr;              // flag0, flag1, dc bits 7..0 (10 bits, first bin highest)
-    uint32_t rem, acc, ret;
-    uint32_t ncorr, ccount, cpos, cneg;
-    uint32_t nent, cap, ovf, bad;
+    uint32_t nent, cap, ovf, bad, ccount;
     int item;
 };
 
@@ -129,7 +130,7 @@ __device__ __forceinline__ uint32_t ctx_bin(LaneState &L, uint32_t *cp) {
     return bit;
 }
 
-// nb bypass bits, 1 <= nb <= 16 (src/mc_codec.c:205,216-226).
+// nb bypass bits read as one batch, 1 <= nb <= 16 (src/mc_codec.c:205,216-226).
 __device__ __forceinline__ uint32_t bypass_bits(LaneState &L, uint32_t nb) {
     L.range >>= nb;
     uint32_t q;
@@ -143,6 +144,25 @@ __device__ __forceinline__ uint32_t bypass_bits(LaneState &L, uint32_t nb) {
     L.code -= q * L.range;
     renorm(L);
     return q;
+}
+
+// Any number of bypass bits: pieces of 16, most significant first
+// (src/mc_codec.c:219-220).
+__device__ __forceinline__ uint32_t bypass_long(LaneState &L, uint32_t nb) {
+    uint32_t v = 0;
+    while (nb > 16) { v = (v << 16) | bypass_bits(L, 16); nb -= 16; }
+    return nb ? (v << nb) | bypass_bits(L, nb) : v;
+}
+
+// Exp-Golomb value in bypass bins (src/mc_codec.c:234-238); a prefix of
+// kEgCap one-bits marks the stream bad and yields 0.
+__device__ __forceinline__ uint32_t eg_value(LaneState &L) {
+    uint32_t nb = 0;
+    while (bypass_bits(L, 1)) {
+        if (++nb >= (uint32_t)kEgCap) { L.bad = 1; return 0; }
+    }
+    if (!nb) return 0;
+    return ((1u << (nb & 31)) | bypass_long(L, nb)) - 1u;
 }
 
 // Appends one entry; false (stream cut short) when a corrupt stream also
@@ -165,15 +185,31 @@ __device__ __forceinline__ bool put_entry(LaneState &L, const EntParams &P, uint
 }
 
 // Context slot of the bin the lane's state asks for next and its current
-// value; bypass states use the scratch slot.
+// value; bypass bins use the scratch slot.
 __device__ __forceinline__ void load_ctx(LaneState &L, const uint32_t *ctx) {
     L.cc = L.st == F_SIG ? L.sigb + min((uint32_t)__popc(L.hist & 0xFFFFu), 3u)
-                         : (L.st == F_MAG ? (uint32_t)kCtxMag + L.k : kSignSlot);
+                         : (L.st == F_MAG ? (uint32_t)kCtxMag + L.k : kScr);
     L.pc = ctx[L.cc * 32];
 }
 
 // flags bit 1 (has corrections) is the second header bin
 __device__ __forceinline__ bool has_corr(const LaneState &L) { return (L.hdr >> 8) & 1; }
+
+// A lane with no more work: a fixed point of fast_step. With code 0, range
+// 0xFFFFF000 and probability 4096 on the scratch slot, every step decodes a
+// 0 that leaves range, probability and selector as they are, so the lane
+// reads nothing, stores nothing and raises no event.
+__device__ __forceinline__ void park(LaneState &L) {
+    L.st = S_IDLE;
+    L.item = -1;
+    L.code = 0;
+    L.range = 0xFFFFF000u;
+    L.pc = 4096;
+    L.cc = kScr;
+    L.sel = kSel0;
+    L.m = 0;
+    L.rem = 0;
+}
 
 // Scan position L.p is current and L.p >= L.stop: a band change and/or the
 // end of the scan. The last position before the EOB is significant by
@@ -208,10 +244,10 @@ __device__ __forceinline__ void lane_begin(LaneState &L, const EntParams &P, uin
     L.cap = entry_cap(L.len);
     L.ovf = 0xFFFFFFFFu;
     L.bad = 0;
-    L.nent = 0; L.ncorr = 0; L.ccount = 0; L.cpos = 0; L.cneg = 0;
+    L.nent = 0;
+    L.ccount = 0;
     L.hdr = 0;
-    L.rem = 0; L.acc = 0; L.ret = R_MAG;
-    L.p = 0; L.eob = 0; L.hist = 0; L.k = 0; L.m = 0;
+    L.p = 0; L.eob = 0; L.hist = 0; L.k = 0; L.m = 0; L.rem = 0; L.acc = 0;
     L.band = 0; L.sigb = kCtxSig; L.bend = s_bend[0]; L.stop = 0;
     if (L.len == 0) { L.st = S_DONE; return; }   // absent block: zeros
     const uint4 *q = reinterpret_cast<const uint4 *>(P.qtab[it.qslot].ctx);
@@ -259,166 +295,229 @@ __device__ __forceinline__ void lane_finish(LaneState &L, const EntParams &P) {
     if (L.bad) atomicAdd(P.status, 1u);
 }
 
-__device__ __forceinline__ void eg_start(LaneState &L, uint32_t ret) {
-    L.st = F_EGP; L.k = kEgBase; L.ret = ret;
-}
-
-__device__ __forceinline__ void eg_return(LaneState &L, const EntParams &P, uint32_t val) {
-    switch (L.ret) {
-    case R_MAG:
-        L.m = 12u + val;              // 11 unary rungs + Exp-Golomb tail + 1
-        L.st = F_SIGN;                // the sign bypass follows
-        break;
-    case R_CCOUNT: {
-        uint32_t n = val + 1u;
-        if (n > (uint32_t)kN3) n = kN3;
-        L.ncorr = n; L.ccount = 0; L.cpos = 0;
-        eg_start(L, R_CGAP);
-        break;
-    }
-    case R_CGAP:
-        L.cpos += val;
-        L.st = S_CSIGN;
-        break;
-    default: {   // R_CMAG
-        const uint32_t m = val + 1u;
-        if (L.cpos >= (uint32_t)kN3) { L.st = S_DONE; break; }
-        if (!put_entry(L, P, L.cpos) || !put_entry(L, P, L.cneg ? 0u - m : m)) break;
+// The sparse max-error corrections after the scan (src/mc_codec.c:770-782):
+// count, then per correction a position gap, a sign and a magnitude, each
+// gap and magnitude an Exp-Golomb value. Recorded as entry pairs (position,
+// wrapping delta) after the coefficients.
+__device__ __forceinline__ void decode_corrections(LaneState &L, const EntParams &P) {
+    uint32_t n = eg_value(L) + 1u;
+    if (L.bad) return;
+    if (n > (uint32_t)kN3) n = kN3;
+    uint32_t pos = 0;
+    for (uint32_t c = 0; c < n; ++c) {
+        pos += eg_value(L);
+        if (L.bad) return;
+        const uint32_t neg = bypass_bits(L, 1);
+        const uint32_t m = eg_value(L) + 1u;
+        if (L.bad || pos >= (uint32_t)kN3) return;
+        if (!put_entry(L, P, pos) || !put_entry(L, P, neg ? 0u - m : m)) return;
         L.ccount++;
-        if (L.ccount == L.ncorr) L.st = S_DONE;
-        else eg_start(L, R_CGAP);
-        break;
-    }
     }
 }
 
-// Slow path: one step of the rare states (src/mc_codec.c:216-238, 770-782).
-__device__ __forceinline__ void slow_step(LaneState &L, const EntParams &P) {
-    const uint32_t st = L.st;
-    if (st == S_END) {
-        if (has_corr(L)) eg_start(L, R_CCOUNT);
-        else L.st = S_DONE;
+// The slow states of one lane, run while the rest of its warp waits.
+__device__ __forceinline__ void slow_work(LaneState &L, const EntParams &P, const uint32_t *ctx,
+                                          const uint16_t *s_bend) {
+    if (L.st == S_EGS) {
+        // a suffix of more than 16 bits: the batched division form in pieces
+        // (src/mc_codec.c:219-224); magnitude 12 + x, x = (1 << nb | suffix) - 1
+        const uint32_t nb = L.rem;
+        const uint32_t m = 11u + ((1u << (nb & 31)) | bypass_long(L, nb));
+        L.rem = 0;
+        L.acc = 0;
+        if (m != 0) {   // the sign follows as a fast bypass bin
+            L.m = m;
+            L.st = F_BYP;
+            load_ctx(L, ctx);
+            return;
+        }
+        // m wrapped to 0 (a corrupt stream only): a zero-level coefficient,
+        // recorded here so that m == 0 keeps meaning "Exp-Golomb prefix"
+        bypass_bits(L, 1);
+        if (!put_entry(L, P, L.p)) return;
+        L.p++;
+        L.st = F_SIG;
+        L.k = 0;
+        if (L.p >= L.stop) position_event(L, ctx, s_bend);
+        else load_ctx(L, ctx);
         return;
     }
-    if (st == S_EGS) {
-        const uint32_t nb = min(L.rem, 16u);
-        L.acc = (L.acc << nb) | bypass_bits(L, nb);
-        L.rem -= nb;
-        if (L.rem == 0) {
-            const uint32_t nbits = L.k - kEgBase;
-            eg_return(L, P, ((1u << (nbits & 31)) | L.acc) - 1u);
-        }
-    } else {      // S_CSIGN
-        L.cneg = bypass_bits(L, 1);
-        eg_start(L, R_CMAG);
-    }
+    // S_END
+    if (has_corr(L)) decode_corrections(L, P);
+    L.st = S_DONE;
 }
 
-// Predicated shared / global stores (one instruction each, no branch).
-__device__ __forceinline__ void sts_if(bool pred, uint32_t *p, uint32_t v) {
-    asm volatile("{.reg .pred q; setp.ne.u32 q, %2, 0; @q st.shared.u32 [%0], %1;}"
-                 :: "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v), "r"((uint32_t)pred) : "memory");
-}
+// Predicated global store (one instruction, no branch).
 __device__ __forceinline__ void stg_if(bool pred, uint32_t *p, uint32_t v) {
     asm volatile("{.reg .pred q; setp.ne.u32 q, %2, 0; @q st.global.u32 [%0], %1;}"
                  :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
 }
 
-// One bin of the coefficient loop. The significance bin of position p uses
-// context band*4 + min(popcount(last 16 significance flags), 3)
-// (src/mc_codec.c:249-259); magnitude rung k context 56+k
-// (src/mc_codec.c:268-275); signs and Exp-Golomb prefix bits are bypass bins
-// (:205,229-238,369) computed by the same instructions with r0 = range/2 and
-// the scratch context slot.
+// The rare events of a fast step, in this order: a window refill, the rest of
+// a renormalisation (none inside an Exp-Golomb suffix), an entry past the
+// block's arena share, the end of an Exp-Golomb prefix (a suffix of nb bits
+// follows: the range loses its low nb bits, which is the batched read's
+// range >> nb, and the suffix bits then halve it, or nb = 0 and the sign
+// follows), the end of a suffix (the magnitude is known; the sign follows),
+// and a scan position at a band change or the end of the scan.
+enum : uint32_t { EV_PFX = 1, EV_PFX_ONE = 2, EV_SFX = 4, EV_OVF = 8, EV_POS = 16 };
+__device__ __forceinline__ void fast_event(LaneState &L, const EntParams &P, const uint32_t *ctx,
+                                           const uint16_t *s_bend, uint32_t why, uint32_t v) {
+    if (L.sel == kSel0 + 4) refill(L);
+    if (!(L.st == F_BYP && L.rem != 0)) renorm(L);
+    if ((why & EV_OVF) && !put_entry(L, P, v)) return;   // corrupt stream: pool exhausted, block ends
+    if (why & EV_PFX) {
+        if (why & EV_PFX_ONE) { L.bad = 1; L.st = S_DONE; return; }   // prefix cap reached (corrupt stream)
+        const uint32_t nb = L.k - kEgBase;                            // one-bits of the prefix
+        if (nb == 0) {
+            L.m = 12;
+        } else if (nb <= 16) {
+            L.rem = nb;
+            L.acc = 0;
+            L.range &= ~((1u << nb) - 1u);
+        } else {
+            L.rem = nb;
+            L.st = S_EGS;
+        }
+    }
+    if (why & EV_SFX) L.m = 11u + ((1u << (L.k - kEgBase)) | L.acc);
+    if (why & EV_POS) position_event(L, ctx, s_bend);
+}
+
+// One bin of every lane. The significance bin of position p uses context
+// band*4 + min(popcount(last 16 significance flags), 3) (src/mc_codec.c:249-259
+// and 353-375); magnitude rung k context 56+k (src/mc_codec.c:268-275); signs
+// and Exp-Golomb bits are bypass bins (:205, 216-238) computed by the same
+// instructions with r0 = range/2 and the scratch context slot. An Exp-Golomb
+// suffix of nb <= 16 bits is the reference's batched read range >>= nb,
+// q = min(code / range, 2^nb - 1), code -= q * range: with the range's low nb
+// bits cleared first, nb halvings without renormalisation between them are
+// that long division bit by bit, clamp included, and leave the same code and
+// range; the renormalisation follows the last bit.
 // The step is software-pipelined: the bin's context value (pc, slot cc) was
 // fetched during the previous step, and this step fetches both candidate
 // contexts of the next bin (one per value of this bin) before it decodes, so
 // the shared-memory round trip overlaps the arithmetic; a next context equal
-// to this bin's takes the freshly updated value instead. The common path is
-// straight-line code of selects and predicated stores, so a warp whose lanes
-// sit in different states issues one instruction stream; rare events (window
-// refill, a second renormalisation byte, band change, end of scan, end of an
-// Exp-Golomb prefix, entry-list overflow) share one branch. A lane in any
-// other state passes through unchanged.
-// INNER: every lane of the warp is live or idle (the first step of an inner
-// loop round). An idle lane's decoder fields are then don't-care -- it never
-// decodes again -- so only its state, its stores and the rare-event branch
-// stay guarded. A lane in a slow state needs every field kept.
-template <bool INNER>
+// to this bin's takes the freshly updated value instead. Every lane runs the
+// same straight-line code of selects and predicated stores; a parked lane
+// passes through unchanged, and lanes in slow states never get here. Rare
+// events (see fast_event) share one branch.
 __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_bend) {
-    const uint32_t st = L.st;
-    const bool live = st <= F_EGP;
-    const bool is_sig = st == F_SIG, is_mag = st == F_MAG, is_sign = st == F_SIGN, is_egp = st == F_EGP;
-    const bool is_byp = is_sign | is_egp;
-    // candidate contexts of the next bin: c0 if this bin is 0, c1 if it is 1
-    const uint32_t k1 = L.k + 1u;
-    // significant flags among the last 16 positions once this bin (if a
-    // significance bin) has come out 0: the window then drops its oldest flag
-    const uint32_t sig_next = L.sigb + min((uint32_t)__popc(L.hist & (is_sig ? 0x7FFFu : 0xFFFFu)), 3u);
-    const uint32_t c0 = (is_sig | is_sign) ? sig_next : kSignSlot;
-    const uint32_t c1 = is_sig ? (uint32_t)kCtxMag
-                               : (is_mag ? (k1 < 12u ? (uint32_t)kCtxMag + k1 : kSignSlot) : c0);
+    const uint32_t st = L.st, m0 = L.m, rem0 = L.rem, k0 = L.k, cc = L.cc, pc = L.pc;
+    const bool is_sig = st == F_SIG, is_mag = st == F_MAG, is_byp = st == F_BYP;
+    const bool is_sign = is_byp & (m0 != 0u);
+    const bool is_sfx = is_byp & (rem0 != 0u);
+    const bool is_pfx = is_byp & !is_sign & !is_sfx;
+    // candidate contexts of the next bin: c0 if this bin is 0, c1 if it is 1.
+    // After a significance bin of 0 the flag window drops its oldest flag.
+    const uint32_t csig = L.sigb + min((uint32_t)__popc(L.hist & (is_sig ? 0x7FFFu : 0xFFFFu)), 3u);
+    const uint32_t c0 = (is_sig | is_sign) ? csig : kScr;
+    const uint32_t c1 = is_sig ? (uint32_t)kCtxMag : (is_mag ? min(cc + 1u, kScr) : c0);
     const uint32_t q0 = ctx[c0 * 32];
     const uint32_t q1 = ctx[c1 * 32];
     // this bin
-    const uint32_t p0 = L.pc;
-    const uint32_t r0 = is_byp ? L.range >> 1 : (L.range >> 12) * p0;
-    const bool bit = (INNER || live) & (L.code >= r0);
-    const uint32_t b = bit ? 1u : 0u;
+    const uint32_t r0 = is_byp ? L.range >> 1 : (L.range >> 12) * pc;
+    const bool bit = L.code >= r0;
     const uint32_t code = bit ? L.code - r0 : L.code;
-    const uint32_t range = !(INNER || live) ? L.range : ((bit & !is_byp) ? L.range - r0 : r0);
-    const uint32_t np0 = p0 + (uint32_t)((int)((bit ? 15u : 4096u) - p0) >> 4);
-    sts_if(live & !is_byp, ctx + L.cc * 32, np0);
-    // renormalisation, first byte (src/mc_codec.c:202)
-    const bool need = range < (1u << 24);
+    const uint32_t range = (bit & !is_byp) ? L.range - r0 : r0;
+    const uint32_t np0 = pc + (uint32_t)((int)((bit ? 15u : 4096u) - pc) >> 4);
+    ctx[cc * 32] = np0;   // bypass bins write the scratch slot
+    // renormalisation, first byte (src/mc_codec.c:202); not between the bits
+    // of a suffix
+    const bool sup = is_sfx & (rem0 > 1u);
+    const bool need = (range < (1u << 24)) & !sup;
     L.code = need ? __byte_perm(code, L.w, L.sel) : code;
     L.range = need ? range << 8 : range;
     L.sel += need ? 1u : 0u;
     // next bin's context
     const uint32_t ncc = bit ? c1 : c0;
-    const uint32_t nq = bit ? q1 : q0;
-    L.pc = (INNER || live) ? ((ncc == L.cc && !is_byp) ? np0 : nq) : L.pc;
-    L.cc = (INNER || live) ? ncc : L.cc;
-
-    // significance history
-    L.hist = is_sig ? (L.hist << 1) | b : L.hist;
-    const uint32_t m = L.m;
-    L.m = is_mag ? k1 : m;
-    const bool esc = is_mag & bit & (L.k == 11);            // 12th rung set: Exp-Golomb tail
-    L.k = (INNER || live) ? (((is_mag | is_egp) & bit) ? k1 : 0u) : L.k;
-    L.ret = esc ? (uint32_t)R_MAG : L.ret;
-    const uint32_t nst = is_sig ? b : (is_mag ? (bit ? (esc ? (uint32_t)F_EGP : (uint32_t)F_MAG) : (uint32_t)F_SIGN)
-                                            : (is_sign ? (uint32_t)F_SIG : (uint32_t)F_EGP));
-    L.st = live ? nst : st;
-    const bool adv = is_sig ? !bit : is_sign;
-    const bool egend = is_egp & (!bit | (k1 >= kEgBase + (uint32_t)kEgCap));
+    L.pc = ncc == cc ? np0 : (bit ? q1 : q0);
+    L.cc = ncc;
+    // state
+    const bool esc = is_mag & bit & (k0 == 11u);   // 12th rung set: Exp-Golomb tail
+    L.hist = is_sig ? (L.hist << 1) | (bit ? 1u : 0u) : L.hist;
+    L.k = is_sig ? 0u : ((bit & !is_sfx) ? k0 + 1u : k0);
+    L.m = (is_mag & !bit) ? k0 + 1u : (is_sign ? 0u : m0);
+    L.acc = is_sfx ? (L.acc << 1) | (bit ? 1u : 0u) : L.acc;
+    L.rem = is_sfx ? rem0 - 1u : rem0;
+    L.st = is_sig ? (bit ? (uint32_t)F_MAG : (uint32_t)F_SIG)
+                  : (is_mag ? ((bit & !esc) ? (uint32_t)F_MAG : (uint32_t)F_BYP) : (is_sign ? (uint32_t)F_SIG : st));
     // a sign completes the coefficient at scan position p: its entry
-    const uint32_t v = L.p | ((bit ? 0u - m : m) << 16);
-    const bool ovf = is_sign & (L.nent >= L.cap);
-    const bool store = is_sign & !ovf;
-    stg_if(store, L.ent + L.nent, v);
-    L.nent += store ? 1u : 0u;
-    const uint32_t np = L.p + (adv ? 1u : 0u);
+    const uint32_t p = L.p;
+    const bool adv = (is_sig & !bit) | is_sign;
+    const uint32_t np = p + (adv ? 1u : 0u);
     L.p = np;
-    const bool event = adv & (np >= L.stop);
-    if (live & ((L.sel == kSel0 + 4) | (L.range < (1u << 24)) | ovf | egend | event)) {
-        if (L.sel == kSel0 + 4) refill(L);
-        renorm(L);
-        if (ovf && !put_entry(L, P, v)) return;   // corrupt stream: pool exhausted, block ends
-        if (egend) {
-            if (bit) { L.bad = 1; L.st = S_DONE; return; }   // prefix cap reached (corrupt stream)
-            const uint32_t nb = k1 - 1u - kEgBase;           // one-bits of the prefix
-            if (nb == 0) eg_return(L, P, 0);
-            else { L.st = S_EGS; L.rem = nb; L.acc = 0; L.k = kEgBase + nb; }
+    const uint32_t v = p | ((bit ? 0u - m0 : m0) << 16);
+    const bool room = L.nent < L.cap;
+    stg_if(is_sign & room, L.ent + L.nent, v);
+    L.nent += (is_sign & room) ? 1u : 0u;
+    const bool pfx_end = is_pfx & (!bit | (k0 + 1u >= kEgBase + (uint32_t)kEgCap));
+    const bool pos = adv & (np >= L.stop);
+    const bool ovf = is_sign & !room;
+    const bool sfx_end = is_sfx & (rem0 == 1u);
+    if ((L.sel == kSel0 + 4) | ((L.range < (1u << 24)) & !sup) | pfx_end | sfx_end | pos | ovf) {
+        const uint32_t why = (pfx_end ? (uint32_t)EV_PFX : 0u) | ((pfx_end & bit) ? (uint32_t)EV_PFX_ONE : 0u) |
+                             (sfx_end ? (uint32_t)EV_SFX : 0u) | (ovf ? (uint32_t)EV_OVF : 0u) |
+                             (pos ? (uint32_t)EV_POS : 0u);
+        fast_event(L, P, ctx, s_bend, why, v);
+    }
+}
+
+// Work queue of a launch: the first ncoded entries of the processing order
+// (longest payload first). Lane g starts with entry g; later entries are
+// claimed from the launch's counter in runs of P.claim consecutive entries.
+struct Claim {
+    int next, end;
+};
+__device__ __forceinline__ int claim_next(Claim &c, const EntParams &P, int nlanes) {
+    if (c.next >= c.end) {
+        const uint32_t run = P.claim > 0 ? (uint32_t)P.claim : 1u;
+        c.next = nlanes + (int)atomicAdd(P.counter, run);
+        c.end = c.next + (int)run;
+    }
+    return c.next++;
+}
+
+// Every lane of the warp decodes blocks until the queue is empty. Fast steps
+// run while every lane is in a fast state or parked; when a lane reaches a
+// slow state the warp leaves the loop, that lane works its slow states off
+// (finishing its block and starting the next one), and the loop resumes.
+// Every block ends after a bounded number of bins (finite scan, capped
+// Exp-Golomb prefixes, bounded correction count) and every lane claims at
+// most ncoded blocks, so the loop ends. on_done(item) runs for every
+// finished block.
+template <class OnDone>
+__device__ __forceinline__ void run_lanes(LaneState &L, const EntParams &P, uint32_t *ctx, const uint16_t *s_bend,
+                                          int gtid, int nlanes, OnDone on_done) {
+    memset(&L, 0, sizeof L);
+    park(L);
+    L.st = S_DONE;
+    Claim c{gtid, gtid + 1};
+    for (;;) {
+        while (!__any_sync(0xFFFFFFFFu, L.st >= S_END)) fast_step(L, P, ctx, s_bend);
+        while (L.st >= S_END) {
+            if (L.st != S_DONE) {
+                slow_work(L, P, ctx, s_bend);
+                continue;
+            }
+            if (L.item >= 0) {
+                lane_finish(L, P);
+                on_done(L.item);
+            }
+            const int nx = claim_next(c, P, nlanes);
+            if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[nx] : nx);
+            else park(L);
         }
-        if (event) position_event(L, ctx, s_bend);
+        if (__all_sync(0xFFFFFFFFu, L.st == S_IDLE)) break;
     }
 }
 
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
-    __shared__ uint16_t s_bend[9];     // s_bend[b]: first scan position past band b
-    __shared__ uint32_t s_ctx[WARPS][kCtxSlots][32];
+    // s_bend[b]: first scan position past band b; then the lanes' contexts,
+    // context j of lane l of warp w at word (w * kCtxSlots + j) * 32 + l
+    extern __shared__ uint32_t s_ent[];
+    uint16_t *s_bend = reinterpret_cast<uint16_t *>(s_ent);
     for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
         const uint32_t b = P.scan[i] >> 12;
         if ((P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
@@ -426,47 +525,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
     if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t *ctx = &s_ctx[warp][0][lane];
-    const int nlanes = gridDim.x * blockDim.x;
-
-    // Work: the first ncoded entries of the processing order (longest payload
-    // first). Each lane starts with one block; later blocks come from a shared
-    // counter as lanes finish, so long and short blocks even out. A lane
-    // without a block holds a valid decoder state that the bin step passes
-    // through unchanged.
+    uint32_t *ctx = s_ent + 8 + warp * kCtxSlots * 32 + lane;
     LaneState L;
-    memset(&L, 0, sizeof L);
-    L.range = 0xFFFFFFFFu;
-    L.sel = kSel0;
-    L.st = S_DONE;
-    L.item = -1;
-    int first = blockIdx.x * blockDim.x + threadIdx.x;
-
-    // Outer loop: block ends and starts, and slow steps of single lanes (the
-    // other lanes take a bin meanwhile). Inner loop: two bins per live lane
-    // per round, for as long as no lane needs the outer loop. Every block ends
-    // after a bounded number of bins (finite scan, capped Exp-Golomb
-    // prefixes), and every lane fetches at most ncoded blocks, so both loops
-    // terminate.
-    for (;;) {
-        const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
-        if (idle == 0xFFFFFFFFu) break;
-        while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
-            fast_step<true>(L, P, ctx, s_bend);    // every lane live or idle here
-            fast_step<false>(L, P, ctx, s_bend);   // the first step may have left a lane in a slow state
-        }
-        fast_step<false>(L, P, ctx, s_bend);
-        if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
-        if (L.st == S_DONE) {
-            if (L.item >= 0) lane_finish(L, P);
-            const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.counter, 1u);
-            first = -1;
-            L.item = -1;
-            if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[nx] : nx);
-            else L.st = S_IDLE;
-        }
-    }
+    run_lanes(L, P, ctx, s_bend, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, [](int) {});
 }
+// dynamic shared memory of k_entropy<W>
+constexpr size_t entropy_smem(int warps) { return 32 + sizeof(uint32_t) * kCtxSlots * 32 * (size_t)warps; }
 
 // ---------------------------------------------------------------- stage 2
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -984,35 +1048,8 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         uint32_t *ctx = &S.u.e.ctx[warp][0][lane];
-        const uint16_t *s_bend = S.u.e.bend;
         LaneState L;
-        memset(&L, 0, sizeof L);
-        L.range = 0xFFFFFFFFu;
-        L.sel = kSel0;
-        L.st = S_DONE;
-        L.item = -1;
-        int first = gtid;
-        for (;;) {
-            const unsigned idle = __ballot_sync(0xFFFFFFFFu, L.st == S_IDLE);
-            if (idle == 0xFFFFFFFFu) break;
-            while (__ballot_sync(0xFFFFFFFFu, L.st > F_EGP) == idle) {
-                fast_step<true>(L, P, ctx, s_bend);    // every lane live or idle here
-                fast_step<false>(L, P, ctx, s_bend);   // the first step may have left a lane in a slow state
-            }
-            fast_step<false>(L, P, ctx, s_bend);
-            if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
-            if (L.st == S_DONE) {
-                if (L.item >= 0) {
-                    lane_finish(L, P);
-                    pair_ready(F, L.item);
-                }
-                const int nx = first >= 0 ? first : nlanes + (int)atomicAdd(P.counter, 1u);
-                first = -1;
-                L.item = -1;
-                if (nx < P.ncoded) lane_begin(L, P, ctx, s_bend, (int)P.order[nx]);
-                else L.st = S_IDLE;
-            }
-        }
+        run_lanes(L, P, ctx, S.u.e.bend, gtid, nlanes, [&F](int item) { pair_ready(F, item); });
     }
     __syncthreads();   // the shared memory changes hands
     rec_init(S.u.r.B);
@@ -1078,23 +1115,21 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
 // decodes one block end to end in one launch, with the work item as a kernel
 // argument -- no batch layout, no host-to-device copies, no second launch.
 // Thread 0 runs the entropy decode through the k_entropy step functions
-// (fast_step pairs, slow_step for the rare states), the CTA then reconstructs
+// (fast_step, slow_work for the rare states), the CTA then reconstructs
 // the block. A branchy scalar loop over the same states was measured slower
 // per bin (p99 block latency 1.23 ms against 0.93): each bin's shared-memory
 // context load and branch resolution then sit on the serial chain, which the
 // warp step avoids by fetching both candidate contexts ahead, without
 // branches.
 
-// The whole stream of one block on one lane: the k_entropy loop with one
-// live lane.
+// The whole stream of one block on one lane: fast steps, and the slow
+// states in between, until the block is done.
 __device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, uint32_t *ctx,
                                              const uint16_t *s_bend) {
-    while (L.st < S_DONE) {
-        while (L.st <= F_EGP) {
-            fast_step<true>(L, P, ctx, s_bend);    // the lane is live here
-            fast_step<false>(L, P, ctx, s_bend);   // the first step may have left it in a slow state
-        }
-        if (L.st < S_DONE) slow_step(L, P);
+    for (;;) {
+        while (L.st <= F_BYP) fast_step(L, P, ctx, s_bend);
+        if (L.st == S_DONE) return;
+        slow_work(L, P, ctx, s_bend);
     }
 }
 
@@ -1147,6 +1182,7 @@ __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, 
         P.scan = scan;
         P.status = status;
         P.counter = nullptr;
+        P.claim = 1;
         uint32_t *ctx = reinterpret_cast<uint32_t *>(sA);
         LaneState L;
         memset(&L, 0, sizeof L);
@@ -1176,14 +1212,33 @@ cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s) {
 
 static int num_sms() { return dev_sms(); }
 
+template <int W>
+static cudaError_t launch_entropy_w(const EntParams &p, int ctas_per_sm, cudaStream_t s) {
+    // per device: the dynamic shared memory opt-in of this instantiation
+    static std::atomic<int> attr[kMaxDevs];
+    const int a = dev_once(attr, [] {
+        const cudaError_t e = cudaFuncSetAttribute(k_entropy<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)entropy_smem(W));
+        return e == cudaSuccess ? 1 : -(int)e;
+    });
+    if (a < 0) return (cudaError_t)(-a);
+    int blocks = (p.ncoded + W * 32 - 1) / (W * 32);
+    const int cap = num_sms() * ctas_per_sm;
+    if (blocks > cap) blocks = cap;
+    k_entropy<W><<<blocks, W * 32, entropy_smem(W), s>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s) {
     if (p.ncoded <= 0) return cudaSuccess;
-    constexpr int W = 4;
-    int blocks = (p.ncoded + W * 32 - 1) / (W * 32);
-    int cap = num_sms() * (cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5);
-    if (blocks > cap) blocks = cap;
-    k_entropy<W><<<blocks, W * 32, 0, s>>>(p);
-    return cudaGetLastError();
+    EntParams q = p;
+    q.claim = cfg.ent_claim > 0 ? cfg.ent_claim : 1;
+    const int per_sm = cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5;
+    switch (cfg.ent_warps) {
+    case 2: return launch_entropy_w<2>(q, per_sm, s);
+    case 8: return launch_entropy_w<8>(q, per_sm, s);
+    default: return launch_entropy_w<4>(q, per_sm, s);
+    }
 }
 
 int fused_grid(const LaunchCfg &cfg) {

@@ -9,7 +9,9 @@ namespace mcb {
 
 // Launch shape knobs, picked per quality by the autotuner.
 struct LaunchCfg {
-    int ent_ctas_per_sm = 5;   // entropy stage: CTAs of 4 warps per SM (<= 5: 44 KB smem)
+    int ent_warps = 4;         // entropy stage: warps per CTA (2, 4 or 8)
+    int ent_claim = 1;         // entropy stage: queue entries a lane claims at a time (1, 2 or 4)
+    int ent_ctas_per_sm = 5;   // entropy stage: CTAs per SM (8.8 KB of contexts per warp)
     int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
     bool split = false;        // long blocks on a second stream (batches large enough to split)
     bool fused = false;        // both stages in one persistent kernel (k_decode_fused)
@@ -35,6 +37,7 @@ struct EntParams {
     const uint16_t *scan;      // scan position -> raster idx | band<<12
     uint32_t *status;          // [0]: blocks whose stream was cut short, [1]: pool entries used
     uint32_t *counter;         // work counter of this launch, zero at launch
+    int claim;                 // queue entries claimed per counter increment (>= 1)
 };
 
 struct RecParams {

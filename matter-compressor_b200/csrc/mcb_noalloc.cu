@@ -214,6 +214,7 @@ extern "C" int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const ui
     ep.scan = reinterpret_cast<const uint16_t *>(sc + kOffScan);
     ep.status = reinterpret_cast<uint32_t *>(sc + kOffStatus);
     ep.counter = ep.status + 2;
+    ep.claim = 1;
     RecParams rp;
     rp.items = ep.items;
     rp.idx = nullptr;

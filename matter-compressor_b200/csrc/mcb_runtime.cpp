@@ -311,6 +311,7 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
         ep.scan = R->d_scan;
         ep.status = status;
         ep.counter = status + 2;
+        ep.claim = cfg.ent_claim > 0 ? cfg.ent_claim : 1;
         RecParams rp;
         rp.items = B.items.as<DecItem>() + i0;
         rp.idx = nullptr;

@@ -1,11 +1,12 @@
 """The entropy stage's device code, compiled for the host and run one lane at
 a time, against the oracle's block decoder.
 
-The lane state machine of k_entropy (lane_begin, fast_step, slow_step,
-lane_finish in csrc/mcb_decode.cu) and the single-block loop of k_decode_one
-are lifted out of the CUDA source, their few device intrinsics replaced by
-host equivalents, and built with g++. Each stream is decoded twice -- by the
-k_entropy loop with one live lane and by the single-block loop -- and both
+The lane state machine of k_entropy (lane_begin, fast_step, fast_event,
+slow_work, lane_finish and the warp loop run_lanes in csrc/mcb_decode.cu) and
+the single-block loop of k_decode_one are lifted out of the CUDA source, their
+few device intrinsics replaced by host equivalents (a warp vote over one lane
+is that lane's own predicate), and built with g++. Each stream is decoded
+twice -- by run_lanes with one lane and by the single-block loop -- and both
 must give the oracle's levels, dc, flags and coefficient count
 (oracle/mc_oracle.c or_dec_block_levels, which follows src/mc_codec.c:739-757,
 353-375). Inputs: the golden block payloads, the corrupt-stream corpus and
@@ -32,6 +33,8 @@ _PRELUDE = r'''#include <stdint.h>
 using std::min;
 template <class T> static T LDG(const T *p) { return *p; }
 static uint32_t ATOMIC_ADD(uint32_t *p, uint32_t v) { uint32_t o = *p; *p += v; return o; }
+static bool ANY_SYNC(unsigned, bool p) { return p; }   // a one-lane warp
+static bool ALL_SYNC(unsigned, bool p) { return p; }
 // __byte_perm: byte n of the result is byte (s >> 4n) & 7 of y:x
 static uint32_t BYTE_PERM(uint32_t x, uint32_t y, uint32_t s) {
     const uint64_t v = ((uint64_t)y << 32) | x;
@@ -42,8 +45,7 @@ static uint32_t BYTE_PERM(uint32_t x, uint32_t y, uint32_t s) {
 namespace mcb {
 '''
 
-_STORES = r'''static inline void sts_if(bool pred, uint32_t *p, uint32_t v) { if (pred) *p = v; }
-static inline void stg_if(bool pred, uint32_t *p, uint32_t v) { if (pred) *p = v; }
+_STORES = r'''static inline void stg_if(bool pred, uint32_t *p, uint32_t v) { if (pred) *p = v; }
 
 '''
 
@@ -82,24 +84,19 @@ extern "C" int emu_block(const uint8_t *pay, uint32_t len, float q, int mode, in
     P.qtab = &qt; P.scan = scan; P.status = status;
     static uint32_t ctx[kCtxSlots * 32];
     LaneState L;
-    memset(&L, 0, sizeof L);
-    lane_begin(L, P, ctx, s_bend, 0);
-    if (mode == 0) {   // the k_entropy loop with one live lane
-        long guard = 0;
-        while (L.st != S_DONE) {
-            while (L.st <= F_EGP) {
-                fast_step<true>(L, P, ctx, s_bend);
-                fast_step<false>(L, P, ctx, s_bend);
-                if (++guard > 100000000) return -1;
-            }
-            fast_step<false>(L, P, ctx, s_bend);
-            if (L.st > F_EGP && L.st < S_DONE) slow_step(L, P);
-            if (++guard > 100000000) return -1;
-        }
+    if (mode == 0) {   // run_lanes, the k_entropy loop, with one lane and a queue of one block
+        uint32_t counter = 0;
+        P.counter = &counter;
+        P.claim = 1;
+        int done = 0;
+        run_lanes(L, P, ctx, s_bend, 0, 1, [&](int) { done++; });
+        if (done != 1) return -1;
     } else {           // k_decode_one's loop
+        memset(&L, 0, sizeof L);
+        lane_begin(L, P, ctx, s_bend, 0);
         solo_entropy(L, P, ctx, s_bend);
+        lane_finish(L, P);
     }
-    lane_finish(L, P);
     memset(levels, 0, 2 * kN3);
     for (uint32_t j = 0; j < hdr.nnz; ++j) {
         const uint32_t e = entries[j];   // arena and pool are contiguous here
@@ -122,13 +119,14 @@ def _host_source():
     src = open(os.path.join(CSRC, "mcb_decode.cu")).read()
     stage1 = _cut(src, "// ---------------------------------------------------------------- stage 1",
                   "template <int WARPS>\n__global__")
-    stores = _cut(stage1, "// Predicated shared / global stores", "// One bin of the coefficient loop.")
+    stores = _cut(stage1, "// Predicated global store", "// The rare events of a fast step")
     stage1 = stage1.replace(stores, _STORES)
     solo = _cut(src, "// The whole stream of one block on one lane", "static_assert(sizeof(DecItem)")
     body = stage1 + solo
     for dev, host in (("__device__ __forceinline__", "static inline"), ("__ldg(", "LDG("),
                       ("atomicAdd(", "ATOMIC_ADD("), ("__byte_perm(", "BYTE_PERM("),
-                      ("__popc(", "__builtin_popcount(")):
+                      ("__popc(", "__builtin_popcount("), ("__any_sync(", "ANY_SYNC("),
+                      ("__all_sync(", "ALL_SYNC(")):
         body = body.replace(dev, host)
     assert "asm" not in body and "__shared__" not in body, "device-only code left in the host build"
     return _PRELUDE + body + "\n}  // namespace mcb\n" + _DRIVER
@@ -190,3 +188,15 @@ def test_random_streams(emu, oracle):
         n = int(rng.integers(0, 600)) if t % 3 else int(rng.integers(600, 16000))
         p = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
         _check(emu, oracle, p, qs[t % len(qs)], f"random {t}")
+
+
+def test_biased_streams(emu, oracle):
+    """Streams of biased random bits (runs of ones): long Exp-Golomb prefixes,
+    suffixes decoded bit by bit, suffixes of more than 16 bits (the batched
+    division path) and prefixes that reach the cap."""
+    rng = np.random.default_rng(5)
+    for t in range(1500):
+        n = int(rng.integers(1, 3000))
+        bias = float(rng.choice([0.5, 0.9, 0.97, 0.995]))
+        p = np.packbits((rng.random(n * 8) < bias).astype(np.uint8)).tobytes()[:n]
+        _check(emu, oracle, p, float(rng.choice([0.5, 1.0, 6.0, 40.0])), f"biased {t}")
