@@ -170,6 +170,11 @@ int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
 typedef struct mc_b200_plan mc_b200_plan;
 mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *chunk_offs, int n,
                                          mc_u8 *d_out, size_t out_stride);
+/* The same for a batch of regions (mc_archive_read_regions' arguments, DEVICE
+ * output: crop i at d_out + i*batch_stride, dense z,y,x): the boxes' blocks,
+ * clipped, decoded and cropped by every replay. */
+mc_b200_plan *mc_b200_plan_read_regions(mc_archive *a, int lod, const mc_box *boxes, int n, long dz, long dy,
+                                        long dx, mc_u8 *d_out, size_t batch_stride);
 /* Replays the plan on `stream` and returns at once. Unlike the other calls,
  * a NULL stream here is the legacy default stream (the graph launch's own
  * meaning of NULL), not the library's per-thread stream. */
@@ -196,6 +201,15 @@ int mc_b200_deblock_dev(mc_u8 *d_vol, int count, size_t vol_stride, int nz, int 
 /* Replace the autotuner's choice (same layout as mc_b200_plan_config) and
  * recapture the plan. 0 on success, -1 on bad arguments or a CUDA error. */
 int  mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]);
+/* The whole launch shape the autotuner chose, which it times on the plan's
+ * own batch (cached per quality and batch size): out[0] entropy warps per CTA
+ * (2, 4, 8), out[1] entropy CTAs per SM, out[2] entropy queue claim run
+ * (entries a lane takes per claim), out[3] reconstruction CTAs per SM,
+ * out[4] the stage layout as in mc_b200_plan_config. */
+void mc_b200_plan_tuning(const mc_b200_plan *p, int out[5]);
+/* Replace it (same layout; warps x CTAs per SM at most 25) and recapture the
+ * plan. 0 on success, -1 on bad arguments or a CUDA error. */
+int  mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[5]);
 /* Fused layout only: how many times (each a sleep of at most 1 us) a CTA
  * polls a completion-list position that no block pair has filled yet before
  * it hands the position to the tail kernel and leaves (default 32768). Any

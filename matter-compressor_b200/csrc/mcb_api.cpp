@@ -140,13 +140,19 @@ struct mc_b200_plan {
 namespace {
 
 std::mutex g_tune_mu;
-std::map<uint32_t, LaunchCfg> g_tuned;   // per quality (bit pattern)
+std::map<uint64_t, LaunchCfg> g_tuned;   // per (quality bit pattern, batch size class)
 
-// Pick CTAs/SM for each stage by timing the real batch (entropy alone, then
-// reconstruction alone) over a small candidate set; cached per quality.
-LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
-    uint32_t key;
-    memcpy(&key, &q, 4);
+// Pick the launch shape of each stage by timing the real batch (entropy
+// alone, then reconstruction alone), then the stage layout; cached per
+// quality and batch size class. Entropy: warps per CTA and CTAs per SM (how
+// many lanes decode at once, and in how many CTAs), then the queue claim run
+// (entries a lane takes per counter increment). Reconstruction: CTAs per SM.
+LaunchCfg autotune(DecodeBatch &B, float q, int nblocks, cudaStream_t s) {
+    uint32_t qb;
+    memcpy(&qb, &q, 4);
+    int size_class = 0;   // batches within a factor of two share a shape
+    while (size_class < 31 && (1 << (size_class + 1)) <= nblocks) ++size_class;
+    const uint64_t key = (uint64_t)qb << 8 | (uint64_t)size_class;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tuned.find(key);
@@ -182,28 +188,27 @@ LaunchCfg autotune(DecodeBatch &B, float q, cudaStream_t s) {
         }
         return total;
     };
-    // two interleaved rounds over the candidates, best time of each counts
-    const int ent_opts[] = {4, 5, 6};
-    const int rec_opts[] = {3, 4, 5};
-    float ent_ms[3] = {1e30f, 1e30f, 1e30f}, rec_ms[3] = {1e30f, 1e30f, 1e30f};
-    for (int round = 0; round < 2; ++round)
-        for (int i = 0; i < 3; ++i) {
-            LaunchCfg c = best;
-            c.ent_ctas_per_sm = ent_opts[i];
-            ent_ms[i] = std::min(ent_ms[i], time_cfg(c, 0));
-        }
-    int be = 0;
-    for (int i = 1; i < 3; ++i) if (ent_ms[i] < ent_ms[be]) be = i;
-    best.ent_ctas_per_sm = ent_opts[be];
-    for (int round = 0; round < 2; ++round)
-        for (int i = 0; i < 3; ++i) {
-            LaunchCfg c = best;
-            c.rec_ctas_per_sm = rec_opts[i];
-            rec_ms[i] = std::min(rec_ms[i], time_cfg(c, 1));
-        }
-    int br = 0;
-    for (int i = 1; i < 3; ++i) if (rec_ms[i] < rec_ms[br]) br = i;
-    best.rec_ctas_per_sm = rec_opts[br];
+    // two interleaved rounds over the candidates of each knob, best time of each counts
+    auto pick = [&](int n, auto set, int stage) {
+        std::vector<float> t(n, 1e30f);
+        for (int round = 0; round < 2; ++round)
+            for (int i = 0; i < n; ++i) {
+                LaunchCfg c = best;
+                set(c, i);
+                t[i] = std::min(t[i], time_cfg(c, stage));
+            }
+        int b = 0;
+        for (int i = 1; i < n; ++i) if (t[i] < t[b]) b = i;
+        set(best, b);
+    };
+    // (warps per CTA, CTAs per SM): 16 to 24 resident warps per SM; 8.8 KB of
+    // contexts per warp bound it at 25
+    static const int ent_shape[][2] = {{4, 4}, {4, 5}, {4, 6}, {2, 8}, {2, 10}, {2, 12}, {8, 2}, {8, 3}};
+    pick(8, [](LaunchCfg &c, int i) { c.ent_warps = ent_shape[i][0]; c.ent_ctas_per_sm = ent_shape[i][1]; }, 0);
+    static const int ent_claim[] = {1, 2, 4};
+    pick(3, [](LaunchCfg &c, int i) { c.ent_claim = ent_claim[i]; }, 0);
+    static const int rec_opts[] = {3, 4, 5};
+    pick(3, [](LaunchCfg &c, int i) { c.rec_ctas_per_sm = rec_opts[i]; }, 1);
     // the whole decode: separate kernels, the long blocks on a second
     // stream, or both stages in one persistent kernel (two rounds, best of each)
     {
@@ -254,6 +259,22 @@ bool plan_capture(mc_b200_plan *p) {
     for (size_t si = 0; si < p->batch.subs.size(); ++si)   // two kernels a sub-batch, four when split
         p->launches += !p->cfg.fused && p->cfg.split && p->batch.split[si] ? 4 : 2;
     return ok;
+}
+
+// A plan over a finished work list: its batch laid out in HBM once, the launch
+// shape autotuned (per quality and batch size), the launches captured.
+mc_b200_plan *plan_build(mc_archive *a, const uint8_t *dbase, const std::vector<DecItem> &items, float q, Lane &L) {
+    mc_b200_plan *p = new mc_b200_plan();
+    p->a = a;
+    p->mirror = dbase;
+    for (const auto &it : items) {
+        p->blocks++;
+        p->payload += it.len;
+    }
+    if (!decode_prepare(p->batch, items.data(), (int)items.size(), L.stream)) { delete p; return nullptr; }
+    p->cfg = autotune(p->batch, q, (int)items.size(), L.stream);
+    if (!plan_capture(p)) { mc_b200_plan_free(p); return nullptr; }
+    return p;
 }
 
 }  // namespace
@@ -582,9 +603,6 @@ mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *offs, in
     if (!L) return nullptr;
     uint8_t *dbase = mirror_sync(a, *L);
     if (!dbase || !finish(*L, nullptr)) return nullptr;
-    mc_b200_plan *p = new mc_b200_plan();
-    p->a = a;
-    p->mirror = dbase;
     std::vector<DecItem> items((size_t)n * kGrid3);
     float q_major = 6.0f;
     for (int c = 0; c < n; ++c) {
@@ -593,17 +611,31 @@ mc_b200_plan *mc_b200_plan_decode_chunks(mc_archive *a, const uint64_t *offs, in
         float q = sanitize_q(chunk_q(a, offs[c]));
         q_major = q;
         int slot = qslot(q);
-        if (slot < 0) { delete p; return nullptr; }
+        if (slot < 0) return nullptr;
         chunk_items(a, offs[c], dbase, slot, dst, &items[(size_t)c * kGrid3]);
     }
-    for (auto &it : items) {
-        p->blocks++;
-        p->payload += it.len;
-    }
-    if (!decode_prepare(p->batch, items.data(), (int)items.size(), L->stream)) { delete p; return nullptr; }
-    p->cfg = autotune(p->batch, q_major, L->stream);
-    if (!plan_capture(p)) { mc_b200_plan_free(p); return nullptr; }
-    return p;
+    return plan_build(a, dbase, items, q_major, *L);
+}
+
+mc_b200_plan *mc_b200_plan_read_regions(mc_archive *a, int lod, const mc_box *boxes, int n, long dz, long dy,
+                                        long dx, mc_u8 *d_out, size_t batch_stride) {
+    if (!a || !boxes || n <= 0 || !d_out || lod < 0 || lod > 7 || dz <= 0 || dy <= 0 || dx <= 0) return nullptr;
+    Lane *L = lane();
+    if (!L) return nullptr;
+    uint8_t *dbase = mirror_sync(a, *L);
+    if (!dbase || !finish(*L, nullptr)) return nullptr;
+    std::vector<DecItem> items;
+    for (int i = 0; i < n; ++i)
+        if (!region_items(a, dbase, lod, boxes[i].z0, boxes[i].y0, boxes[i].x0, dz, dy, dx,
+                          d_out + (size_t)i * batch_stride, (int64_t)dy * dx, dx, items))
+            return nullptr;
+    if (items.empty()) return nullptr;
+    // the quality the most blocks are coded at picks the tuned shape
+    std::map<uint16_t, size_t> per_slot;
+    for (const auto &it : items) per_slot[it.qslot] += it.len != 0;
+    uint16_t major = items[0].qslot;
+    for (const auto &kv : per_slot) if (kv.second > per_slot[major]) major = kv.first;
+    return plan_build(a, dbase, items, slot_quality(major), *L);
 }
 
 int mc_b200_plan_launch(mc_b200_plan *p, void *stream) {
@@ -649,6 +681,36 @@ int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
     c.fused = cfg[2] == 2;
     if (c.fused && fused_grid(c) <= 0) {
         set_error("plan_set_config: the fused kernel cannot launch on this device");
+        return -1;
+    }
+    p->cfg = c;
+    return plan_capture(p) ? 0 : -1;
+}
+
+void mc_b200_plan_tuning(const mc_b200_plan *p, int out[5]) {
+    if (!out) return;
+    out[0] = p ? p->cfg.ent_warps : 0;
+    out[1] = p ? p->cfg.ent_ctas_per_sm : 0;
+    out[2] = p ? p->cfg.ent_claim : 0;
+    out[3] = p ? p->cfg.rec_ctas_per_sm : 0;
+    out[4] = p ? (p->cfg.fused ? 2 : (int)p->cfg.split) : 0;
+}
+
+int mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[5]) {
+    if (!p || !cfg || (cfg[0] != 2 && cfg[0] != 4 && cfg[0] != 8) || cfg[1] < 1 || cfg[0] * cfg[1] > 25 ||
+        cfg[2] < 1 || cfg[2] > 64 || cfg[3] < 1 || cfg[3] > 16 || cfg[4] < 0 || cfg[4] > 2) {
+        set_error("plan_set_tuning: bad arguments");
+        return -1;
+    }
+    LaunchCfg c = p->cfg;
+    c.ent_warps = cfg[0];
+    c.ent_ctas_per_sm = cfg[1];
+    c.ent_claim = cfg[2];
+    c.rec_ctas_per_sm = cfg[3];
+    c.split = cfg[4] == 1;
+    c.fused = cfg[4] == 2;
+    if (c.fused && fused_grid(c) <= 0) {
+        set_error("plan_set_tuning: the fused kernel cannot launch on this device");
         return -1;
     }
     p->cfg = c;

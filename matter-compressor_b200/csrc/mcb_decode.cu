@@ -709,8 +709,13 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
     uint64_t nbase = 0;
     uint32_t nlines = 0;
     if (next >= 0 && tid < 32) {
+        // the entries it reads: coefficients and correction pairs, at most 512
         nbase = __ldg(P.base + next);
-        nlines = (min(entry_cap(__ldg(&P.items[next].len)), 512u) + 31) / 32;   // 128-byte lines
+        const uint4 hv = __ldg(reinterpret_cast<const uint4 *>(P.hdr + next));
+        EntHdr hn;
+        memcpy(&hn, &hv, sizeof hn);
+        const uint32_t used = min((uint32_t)hn.nnz + 2u * hn.ncorr, entry_cap(__ldg(&P.items[next].len)));
+        nlines = (min(used, 512u) + 31) / 32;   // 128-byte lines
     }
     const DecItem it = P.items[item];
     const EntHdr h = load_hdr<CG>(P.hdr + item);

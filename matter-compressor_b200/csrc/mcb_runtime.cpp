@@ -125,6 +125,17 @@ int qslot(float q) {
     return slot;
 }
 
+float slot_quality(int slot) {
+    Runtime *R = runtime();
+    if (!R) return 6.0f;
+    std::lock_guard<std::mutex> g(R->qmu);
+    if (slot < 0 || (size_t)slot >= R->qkeys.size()) return 6.0f;
+    const uint32_t qb = (uint32_t)(R->qkeys[slot] >> 32);
+    float q;
+    memcpy(&q, &qb, 4);
+    return q;
+}
+
 // ------------------------------------------------------------------ lanes
 Lane::~Lane() {
     if (done) cudaEventDestroy(done);

@@ -56,6 +56,8 @@ struct Runtime {
 Runtime *runtime();
 // Device table slot for a (sanitised) quality under the active priors.
 int qslot(float q);
+// The quality a slot was made for (6 for a slot not in use).
+float slot_quality(int slot);
 
 // Device-side state of one batched decode: items, arena offsets, entropy
 // headers, arena and overflow pool. decode_prepare sizes the buffers for the

@@ -114,6 +114,9 @@ class McLib:
                 "mc_b200_plan_config": (None, [vp, vp]),
                 "mc_b200_plan_set_config": (i, [vp, vp]),
                 "mc_b200_plan_set_fused_wait": (i, [vp, u32]),
+                "mc_b200_plan_tuning": (None, [vp, vp]),
+                "mc_b200_plan_set_tuning": (i, [vp, vp]),
+                "mc_b200_plan_read_regions": (vp, [vp, i, vp, i, lg, lg, lg, vp, sz]),
                 "mc_b200_deblock_dev": (i, [vp, i, sz, i, i, i, f, vp]),
                 "mc_b200_decimate_dev": (i, [vp, i, i, i, vp, vp]),
                 "mc_b200_verify_archive_dev": (lg, [vp, vp, sz, i]),
@@ -381,6 +384,18 @@ class Archive:
             raise RuntimeError("plan build failed")
         return Plan(self.lib, p)
 
+    def plan_regions(self, lod, boxes, dz, dy, dx, d_out, batch_stride=None):
+        """A graph-captured decode plan of a read_regions batch into device memory."""
+        n = len(boxes)
+        arr = (McBox * n)(*[McBox(*b) for b in boxes])
+        stride = dz * dy * dx if batch_stride is None else batch_stride
+        p = self.L.mc_b200_plan_read_regions(self.a, lod, C.cast(arr, C.c_void_p), n, dz, dy, dx, C.c_void_p(d_out),
+                                             stride)
+        self.lib.check()
+        if not p:
+            raise RuntimeError("region plan build failed")
+        return Plan(self.lib, p)
+
 
 class Plan:
     def __init__(self, lib, handle):
@@ -408,6 +423,20 @@ class Plan:
                 "stages": ("sequential", "long_blocks_on_second_stream", "fused")[int(out[2])]}
 
     STAGES = ("sequential", "long_blocks_on_second_stream", "fused")
+
+    def tuning(self):
+        """The autotuner's full choice (mc_b200_plan_tuning)."""
+        out = np.zeros(5, np.int32)
+        self.lib.L.mc_b200_plan_tuning(self.p, _ptr(out))
+        return {"entropy_warps_per_cta": int(out[0]), "entropy_ctas_per_sm": int(out[1]),
+                "entropy_claim": int(out[2]), "reconstruct_ctas_per_sm": int(out[3]),
+                "stages": self.STAGES[int(out[4])]}
+
+    def set_tuning(self, warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, stages):
+        cfg = np.array([warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, self.STAGES.index(stages)], np.int32)
+        rc = self.lib.L.mc_b200_plan_set_tuning(self.p, _ptr(cfg))
+        self.lib.check()
+        return rc
 
     def set_config(self, entropy_ctas_per_sm, reconstruct_ctas_per_sm, stages):
         """Override the autotuned launch shape and recapture the plan."""

@@ -277,3 +277,65 @@ def test_fused_layout_gives_up_waiting(gpu, oracle, tmp_path):
                 assert np.array_equal(d_out.cpu().numpy(), want), polls
         finally:
             plan.free()
+
+
+def test_plan_entropy_shapes(gpu, oracle, tmp_path):
+    """Every entropy launch shape the autotuner may pick -- 2, 4 or 8 warps per
+    CTA, several CTAs per SM, queue claims of 1, 2 or 4 entries -- gives the
+    oracle's voxels, at three qualities in one batch."""
+    import torch
+    import volumes
+    with gpu.open(str(tmp_path / "e.mca"), 768, 256, 256, 6.0) as a:
+        for c, q in enumerate((6.0, 1.0, 12.0)):
+            v = volumes.region(61 + c, (0, 0, 256 * c), (256, 256, 256), 0.35, device="cuda").cpu().numpy()
+            assert a.append_par(0, 0, 0, c, v, q) == 0
+        offs = [a.chunk_offset(0, 0, 0, c) for c in range(3)]
+        data = np.fromfile(str(tmp_path / "e.mca"), np.uint8).tobytes()
+        want = np.concatenate([oracle.decode_chunk(data[o:o + shapes.blob_len(data, o)]) for o in offs])
+        d_out = torch.empty(3 * CHUNK, dtype=torch.uint8, device="cuda")
+        plan = a.plan_chunks(offs, d_out.data_ptr())
+        try:
+            t = plan.tuning()
+            assert t["entropy_warps_per_cta"] in (2, 4, 8) and t["entropy_claim"] in (1, 2, 4)
+            for warps, ctas, claim in ((2, 12, 1), (4, 5, 2), (8, 3, 4), (4, 1, 1), (2, 3, 64)):
+                assert plan.set_tuning(warps, ctas, claim, 4, "sequential") == 0
+                assert plan.tuning()["entropy_warps_per_cta"] == warps
+                d_out.fill_(0xEE)
+                plan.launch()
+                torch.cuda.synchronize()
+                assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim)
+            assert plan.set_tuning(3, 4, 1, 4, "sequential") == -1   # 3 warps per CTA: refused
+        finally:
+            plan.free()
+
+
+def test_region_plan(gpu, tmp_path):
+    """A graph-captured plan of a region batch (boxes across chunk borders,
+    into absent chunks and past the volume, strided output) gives what
+    mc_b200_read_regions_dev and the host read_regions give, replay after
+    replay, and leaves the gaps between crops untouched."""
+    import torch
+    with gpu.open(str(tmp_path / "rp.mca"), 1024, 1024, 1024, 6.0) as a:
+        for st in shapes.archive_sequence()[:2]:
+            assert a.append_par(0, *st["at"], shapes.chunk_source(st["src"]), st["q"]) == 0
+        boxes = [(0, 0, 0), (10, 20, 30), (60, 100, 200), (64, 64, 300), (-8, 250, 1000), (200, 200, 450)]
+        dz, dy, dx = 48, 64, 80
+        crop = dz * dy * dx
+        stride = crop + 1000
+        want = torch.full((stride * len(boxes),), 0x5A, dtype=torch.uint8, device="cuda")
+        assert a.read_regions_dev(0, boxes, dz, dy, dx, want.data_ptr(), stride) == 0
+        got = torch.full_like(want, 0x5A)
+        plan = a.plan_regions(0, boxes, dz, dy, dx, got.data_ptr(), stride)
+        try:
+            for _ in range(3):
+                plan.launch()
+            torch.cuda.synchronize()
+        finally:
+            plan.free()
+        assert torch.equal(got, want)
+        g = got.cpu().numpy()
+        for i in range(len(boxes)):
+            assert np.all(g[i * stride + crop:(i + 1) * stride] == 0x5A)
+        host = a.read_regions(0, boxes, dz, dy, dx, batch_stride=stride)
+        for i in range(len(boxes)):
+            assert np.array_equal(g[i * stride:i * stride + crop], host[i * stride:i * stride + crop]), boxes[i]
