@@ -23,6 +23,7 @@ Multi-GPU: python -m torch.distributed.run --nproc-per-node N bench.py --gpus N
 (weak scaling: every rank decodes its own 64 chunks; no data-path collective).
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -58,6 +59,9 @@ def parse():
     p.add_argument("--chunks", type=int, default=64)
     p.add_argument("--q", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--q-sweep", action="store_true",
+                   help="decode: one JSON line per quality in 1, 3, 6, 12 (each with its autotuned launch shape "
+                        "and the reference's CPU decode of the same archive)")
     p.add_argument("--workload", default="decode", choices=["decode", "serve", "regions", "encode", "deblock", "pyramid"],
                    help="decode: batched chunk decode (the headline line); serve: request-serving sweep; "
                         "regions: dataloader region batch; encode: preset-ladder batched encode; "
@@ -173,6 +177,45 @@ def reference_decode(path, nchunks, q, steps, warmup, min_seconds=0.0):
     cores = min(os.cpu_count() or 4, 16)   # the reference's thread cap (src/mc_archive.c:805-809)
     gbs = nchunks * CHUNK / statistics.mean(times) / 1e9
     return gbs, cores, done, times
+
+
+def block_latency(a, offs, picks, skip=20):
+    """ms per mc_archive_decode_block call on (chunk, block) picks; the first
+    `skip` calls warm up."""
+    out = np.empty(4096, np.uint8)
+    dst = C.c_void_p(out.ctypes.data)
+    lat = []
+    for c, bi in picks:
+        t0 = time.perf_counter()
+        a.L.mc_archive_decode_block(a.a, offs[c], bi >> 8, (bi >> 4) & 15, bi & 15, dst)
+        lat.append((time.perf_counter() - t0) * 1e3)
+    return lat[skip:]
+
+
+def plain_chunk_blocks_ms(a, co):
+    """ms for 4096 mc_archive_decode_block calls covering one chunk."""
+    out = np.empty(4096, np.uint8)
+    dst = C.c_void_p(out.ctypes.data)
+    for bi in range(64):   # warm
+        a.L.mc_archive_decode_block(a.a, co, bi >> 8, (bi >> 4) & 15, bi & 15, dst)
+    t0 = time.perf_counter()
+    for bi in range(4096):
+        a.L.mc_archive_decode_block(a.a, co, bi >> 8, (bi >> 4) & 15, bi & 15, dst)
+    return (time.perf_counter() - t0) * 1e3
+
+
+def reference_block_latency(path, nchunks, q, picks):
+    """The reference's own decode_block on the same blocks, and its plain
+    4096-call pass over chunk 0 (one host thread, default-flag build)."""
+    from mcb200 import McLib
+    from oracle import REF_FAST_LIB
+    ref = McLib(REF_FAST_LIB, b200=False)
+    ref.L.mc_codec_init()
+    with ref.open(path, 256 * nchunks, 256, 256, q) as r:
+        offs = [r.chunk_offset(0, 0, 0, c) for c in range(nchunks)]
+        lat = block_latency(r, offs, picks)
+        plain = plain_chunk_blocks_ms(r, offs[0])
+    return lat, plain
 
 
 def build_reference_archive(path, vox_host, q):
@@ -322,8 +365,31 @@ def run_regions(args):
         a.read_regions_dev(0, boxes, 128, 128, 128, d_out.data_ptr(), stride, s.cuda_stream)
         e1.record(s)
     torch.cuda.synchronize()
-    ms = statistics.median([e0.elapsed_time(e1) for e0, e1 in ev])
+    per_call_ms = statistics.median([e0.elapsed_time(e1) for e0, e1 in ev])
     dev = d_out.cpu().numpy()
+    # the same batch as a graph-captured plan (work list, batch layout and
+    # launch shape built once), replayed per step
+    d_plan = torch.zeros_like(d_out)
+    plan = a.plan_regions(0, boxes, 128, 128, 128, d_plan.data_ptr(), stride)
+    plan_cfg = plan.tuning()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        plan.launch(s.cuda_stream)
+    torch.cuda.synchronize()
+    pt = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        plan.launch(s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        pt.append(e0.elapsed_time(e1))
+    ms = statistics.median(pt)
+    plan_exact = bool(torch.equal(d_plan, d_out))
+    _, plan_blocks, _ = plan.info()
+    plan.free()
+    del flush
     # plain drop-in, host output
     t0 = time.perf_counter()
     host = a.read_regions(0, boxes, 128, 128, 128, batch_stride=stride)
@@ -382,6 +448,15 @@ def run_regions(args):
                                    f"q={args.q:g}, {nch} chunks, into a strided device batch",
                        "boxes": len(boxes), "batch_stride": stride},
             "bit_exact_device_vs_host_call": exact, "bit_exact_vs_reference_strict_build": exact_ref,
+            "bit_exact_plan_vs_per_call": plan_exact,
+            "api": "mc_b200_plan_read_regions + mc_b200_plan_launch (graph replay; L2 flushed between steps)",
+            "launch_config": plan_cfg, "blocks_per_step": plan_blocks,
+            "per_call": {"api": "mc_b200_read_regions_dev (work list built per call)", "ms": round(per_call_ms, 4),
+                         "gbs": round(len(boxes) * crop / 1e9 / (per_call_ms / 1e3), 3)},
+            "roofline": {"bound": "hbm", "achieved": round(len(boxes) * crop / 1e9 / (ms / 1e3), 3),
+                         "peak": hbm_peak()[0], "peak_kind": hbm_peak()[1], "unit": "GB/s",
+                         "frac": round(len(boxes) * crop / 1e9 / (ms / 1e3) / hbm_peak()[0], 4),
+                         "algorithmic_bytes": "crop bytes written"},
             "plain_host_call": {"api": "mc_archive_read_regions (host output)", "ms": round(host_ms, 3),
                                 "gbs": round(gb / (host_ms / 1e3), 3)},
             "verify": verify,
@@ -740,7 +815,7 @@ def run_b200(args, d):
     out = torch.empty(args.chunks * CHUNK, dtype=torch.uint8, device=dev)
     plan = a.plan_chunks(offs, out.data_ptr())
     launches_per_step, blocks, payload = plan.info()
-    plan_cfg = plan.config()
+    plan_cfg = plan.tuning()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     s = torch.cuda.current_stream()
     for w in range(args.warmup):
@@ -784,8 +859,10 @@ def run_b200(args, d):
     # the whole decode under each stage layout the autotuner chose among,
     # its entropy and reconstruction shapes kept (the chosen layout is the step above)
     layout_ms = {}
+    tuned = [plan_cfg[k] for k in ("entropy_warps_per_cta", "entropy_ctas_per_sm", "entropy_claim",
+                                   "reconstruct_ctas_per_sm")]
     for stages in plan.STAGES:
-        if plan.set_config(plan_cfg["entropy_ctas_per_sm"], plan_cfg["reconstruct_ctas_per_sm"], stages) != 0:
+        if plan.set_tuning(*tuned, stages) != 0:
             continue
         for k in range(2):
             plan.launch(s.cuda_stream)
@@ -799,7 +876,7 @@ def run_b200(args, d):
             torch.cuda.synchronize()
             tot += e0.elapsed_time(e1)
         layout_ms[stages] = round(tot / args.steps, 4)
-    plan.set_config(plan_cfg["entropy_ctas_per_sm"], plan_cfg["reconstruct_ctas_per_sm"], plan_cfg["stages"])
+    plan.set_tuning(*tuned, plan_cfg["stages"])
     plan.launch(s.cuda_stream)
     torch.cuda.synchronize()
 
@@ -811,14 +888,12 @@ def run_b200(args, d):
         exact = bool(np.array_equal(out[:CHUNK].cpu().numpy(), Oracle().decode_chunk(blob)))
 
     # plain per-call drop-in latency: mc_archive_decode_block on random blocks
+    # (the reference's own decode_block times the same blocks below)
     rng = np.random.Generator(np.random.PCG64(d.rank))
-    lat = []
-    for _ in range(300):
-        c, bi = int(rng.integers(0, args.chunks)), int(rng.integers(0, 4096))
-        t0 = time.perf_counter()
-        a.decode_block(offs[c], bi >> 8, (bi >> 4) & 15, bi & 15)
-        lat.append((time.perf_counter() - t0) * 1e3)
-    lat = sorted(lat[20:])
+    picks = [(int(rng.integers(0, args.chunks)), int(rng.integers(0, 4096))) for _ in range(320)]
+    lat = block_latency(a, offs, picks)
+    # config 1's plain method: all 4096 blocks of one chunk, one decode_block call each
+    plain_ms = plain_chunk_blocks_ms(a, offs[0])
 
     # e2e: host blobs (pinned) -> host voxels (pinned) through the C ABI
     blobs = blobs_of(path, offs)
@@ -851,6 +926,12 @@ def run_b200(args, d):
     plan.free()
     a.close()
 
+    ref_lat = ref_plain_ms = None
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_lat, ref_plain_ms = reference_block_latency(path, args.chunks, args.q, picks)
+        except (FileNotFoundError, OSError):
+            pass
     cpu = None
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         try:
@@ -887,8 +968,16 @@ def run_b200(args, d):
                      "traffic": traffic, "algorithmic_bytes_per_launch": args.chunks * CHUNK,
                      "kernel_ms": round(ent_ms, 4), "reconstruct_ms": round(stage_ms[1], 4),
                      "step_frac": round(value / d.world / peak, 4)},
-        "latency": {"api": "mc_archive_decode_block (plain per-call drop-in, host buffer)",
-                    "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[int(len(lat) * 0.99) - 1], 4)},
+        "latency": {"api": "mc_archive_decode_block (plain per-call drop-in, host buffer), 300 random blocks",
+                    "p50_ms": round(pct(lat, 50), 4), "p99_ms": round(pct(lat, 99), 4),
+                    "reference_p50_ms": None if ref_lat is None else round(pct(ref_lat, 50), 4),
+                    "reference_p99_ms": None if ref_lat is None else round(pct(ref_lat, 99), 4),
+                    "reference": "the reference's own mc_archive_decode_block (default-flag build, one host thread) "
+                                 "on the same blocks of the same archive file"},
+        "plain_chunk_decode": {"what": "4096 x mc_archive_decode_block over one 256^3 chunk (config 1's plain method)",
+                               "gpu_ms": round(plain_ms, 3), "gpu_gbs": round(CHUNK / plain_ms / 1e6, 4),
+                               "reference_ms": None if ref_plain_ms is None else round(ref_plain_ms, 3),
+                               "reference_gbs": None if ref_plain_ms is None else round(CHUNK / ref_plain_ms / 1e6, 4)},
         "blocks_per_step": blocks, "payload_bytes_per_step": payload, "launch_config": plan_cfg,
         "stage_layout_ms": layout_ms,
         "clocks": clk,
@@ -905,6 +994,14 @@ def main():
                 raise SystemExit("the serve / regions / encode / deblock / pyramid workloads run on one GPU")
             res = {"serve": run_serve, "regions": run_regions, "encode": run_encode,
                    "deblock": run_deblock, "pyramid": run_pyramid}[args.workload](args)
+        elif args.q_sweep:
+            for q in (1.0, 3.0, 6.0, 12.0):
+                args.q = q
+                res = run_reference(args, d) if args.impl == "reference" else run_b200(args, d)
+                if res is not None:
+                    print(json.dumps(res), flush=True)
+                torch.cuda.empty_cache()
+            res = None
         else:
             res = run_reference(args, d) if args.impl == "reference" else run_b200(args, d)
         if res is not None:
