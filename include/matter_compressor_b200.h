@@ -275,8 +275,11 @@ int mc_b200_append_pyramid(mc_archive *a, const mc_u8 *d_vol, int nz, int ny, in
  * submit; a worker thread admits them into a batch while the batch's output
  * bytes stay within batch_bytes and their missing blocks find free cache
  * slots, decodes the misses into the cache, gathers every request's blocks
- * into its output and completes the tickets. Eviction is FIFO over slots no
- * batch in flight is using. Results are byte-identical to
+ * into its output and completes the tickets. Small requests (up to 256 KiB
+ * of output: blocks, small regions) and large ones queue and batch apart, on
+ * a high-priority and a normal CUDA stream, so a block never waits for a
+ * chunk decode in its own batch. Eviction is FIFO over slots no batch in
+ * flight is using. Results are byte-identical to
  * mc_archive_decode_block / read_region / decode_chunk.
  *
  * out_on_device: request outputs are DEVICE pointers (any strides for

@@ -9,15 +9,24 @@
 // batches:
 //
 //   submit()  queues a request and returns a ticket;
-//   worker    forms a batch from the queue head while the batch's output bytes
+//   worker    forms a batch from a queue head while the batch's output bytes
 //             stay within the batch budget and its missing blocks find free
 //             cache slots (admission by memory), decodes the batch's misses
 //             straight into their cache slots (one entropy + one
 //             reconstruction launch), gathers every request's blocks from the
 //             cache into its output (one launch), and marks the tickets done
-//             from a stream callback. Two batches are in flight at most: while
-//             one runs on the GPU the next is formed from the requests that
-//             arrived meanwhile.
+//             from a stream callback.
+//
+// Requests travel in two classes, each with its own queue, its own CUDA
+// stream and two batches in flight at most: small requests (a block, a small
+// region) on a high-priority stream, large ones (regions over 256 KiB of
+// output, chunks) on a normal one. A block request therefore never waits
+// behind a chunk's decode in the same batch, and the GPU runs a small batch's
+// work ahead of a large batch's queued kernels. The classes share the cache:
+// a batch that reads a chunk whose misses a batch of the other class is still
+// decoding waits on that batch's decode event first, so a block is never read
+// before it is written; slots of chunks that any batch in flight holds are
+// never evicted.
 //
 // Results equal the plain decode paths byte for byte: a cached block is the
 // block decoded by the same kernels, and an absent or out-of-range block reads
@@ -48,6 +57,9 @@ using namespace mcb;
 namespace {
 
 constexpr size_t kChunkBytes = (size_t)256 * 256 * 256;
+// requests with at most this many output bytes go to the small class
+constexpr size_t kSmallBytes = (size_t)256 << 10;
+constexpr int kClasses = 2, kBatchesPerClass = 2;
 
 uint64_t now_ns() {
     return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -62,12 +74,15 @@ struct Ticket {
 // Cache bookkeeping of one chunk blob (keyed by its archive offset): the
 // cache slot of each of its blocks, mirrored in a device table the gather
 // reads. kEmptySlot: not resolved yet; kZeroSlot: an absent block.
+struct SrvBatch;
 struct ChunkRes {
     uint64_t co = 0;
     uint32_t table = 0;
     uint32_t resolved = 0, resident = 0, pins = 0;
     uint64_t pin_seq = 0, last_use = 0;
     int qslot = -1;
+    SrvBatch *dec_batch = nullptr;   // the last batch that decoded misses of this chunk
+    uint64_t dec_seq = 0;            // ... and its sequence number then
     uint32_t slot[kGrid3];
 };
 
@@ -86,6 +101,9 @@ struct SrvBatch {
     size_t staged = 0;                        // staging bytes (host outputs)
     bool busy = false, gpu_done = false;
     uint64_t seq = 0;
+    int cls = 0;                              // request class (stream) of the batch
+    cudaEvent_t decoded = nullptr;            // recorded once the batch's misses are in the cache
+    std::vector<cudaEvent_t> waits;           // decode events of other-class batches it reads after
     struct mc_b200_server *srv = nullptr;
 };
 
@@ -112,13 +130,16 @@ struct mc_b200_server {
     std::mutex mu;
     std::condition_variable cv;        // the worker: new requests, finished batches, close
     std::condition_variable cv_done;   // callers waiting for tickets
-    std::deque<mc_b200_request> queue_req;
-    std::deque<long> queue_tk;
+    std::deque<mc_b200_request> queue_req[kClasses];
+    std::deque<long> queue_tk[kClasses];
     std::deque<Ticket> tickets;
-    SrvBatch batch[2];
+    SrvBatch batch[kClasses][kBatchesPerClass];
+    cudaStream_t stream[kClasses] = {nullptr, nullptr};
+    cudaEvent_t mirror_ev = nullptr;   // the archive mirror's last sync on the worker's lane stream
     uint64_t seq = 0;
     bool stop = false;
-    bool head_blocked = false;   // the queue head waits for cache slots held by a batch in flight
+    bool waiting = false;              // the worker sleeps on cv
+    bool head_blocked[kClasses] = {false, false};   // a queue head waits for cache slots held by a batch in flight
     std::thread worker;
     // statistics
     uint64_t st_req = 0, st_batches = 0, st_blocks = 0, st_hits = 0, st_miss = 0, st_zero = 0, st_evict = 0,
@@ -133,6 +154,14 @@ size_t out_bytes(const mc_b200_request &r) {
     case MC_B200_REQ_CHUNK: return kChunkBytes;
     default: return (size_t)r.dz * r.dy * r.dx;
     }
+}
+
+int class_of(const mc_b200_request &r) { return out_bytes(r) <= kSmallBytes ? 0 : 1; }
+
+bool queues_empty(const mc_b200_server *S) {
+    for (int c = 0; c < kClasses; ++c)
+        if (!S->queue_req[c].empty()) return false;
+    return true;
 }
 
 // One chunk's share of a request, before cache resolution.
@@ -260,7 +289,11 @@ ChunkRes *chunk_res(mc_b200_server *S, uint64_t co) {
 // on the device: buffers grow in launch(), outside the lock that the completion
 // callback takes.
 void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
+    const int cls = B.cls;
+    std::deque<mc_b200_request> &qr = S->queue_req[cls];
+    std::deque<long> &qt = S->queue_tk[cls];
     B.gather.clear();
+    B.waits.clear();
     B.miss.clear();
     B.upd.swap(S->pending_upd);   // writes left over from an empty batch go first
     S->pending_upd.clear();
@@ -274,9 +307,9 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
     std::vector<Piece> ps;
     std::vector<std::pair<ChunkRes *, uint32_t>> misses;   // (chunk, block) to decode
     size_t bytes = 0, staged = 0;
-    while (!S->queue_req.empty()) {
-        const mc_b200_request r = S->queue_req.front();
-        const long t = S->queue_tk.front();
+    while (!qr.empty()) {
+        const mc_b200_request r = qr.front();
+        const long t = qt.front();
         const size_t nb = out_bytes(r);
         if (!B.tickets.empty() && bytes + nb > S->batch_bytes) break;
         // host outputs land in the batch's staging buffer (offsets until launch)
@@ -298,6 +331,11 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
             }
             pin_chunk(S, B, c);   // keeps the chunk's table and slots while the batch forms
             c->last_use = ++S->use_clock;
+            // misses of this chunk still being decoded by a batch of the other class
+            SrvBatch *db = c->dec_batch;
+            if (db && db->busy && db->cls != cls && db->seq == c->dec_seq &&
+                std::find(B.waits.begin(), B.waits.end(), db->decoded) == B.waits.end())
+                B.waits.push_back(db->decoded);
             p.g.table = c->table;
             if (c->resolved == (uint32_t)kGrid3) continue;
             const ChunkIndex &ix = chunk_index(a->base, co);
@@ -319,12 +357,12 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
         }
         if (fail || misses.size() > S->nslots) {   // cannot be served
             S->tickets[t].state = -1;
-            S->queue_req.pop_front();
-            S->queue_tk.pop_front();
+            qr.pop_front();
+            qt.pop_front();
             continue;
         }
         if (no_table || misses.size() > S->nslots - S->pinned_slots) {
-            if (B.tickets.empty()) S->head_blocked = true;   // wait until a batch in flight retires
+            if (B.tickets.empty()) S->head_blocked[cls] = true;   // wait until a batch in flight retires
             break;
         }
         for (auto &m : misses) {
@@ -338,6 +376,8 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
             S->pinned_slots++;   // c is pinned by this batch
             S->slot_owner[s] = c;
             S->slot_block[s] = (uint16_t)bi;
+            c->dec_batch = &B;
+            c->dec_seq = B.seq;
             B.upd.push_back(make_uint2(c->table * kGrid3 + bi, s));
             const ChunkIndex &ix = chunk_index(a->base, c->co);
             DecItem d;
@@ -370,12 +410,13 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
         }
         bytes += nb;
         B.tickets.push_back(t);
-        S->queue_req.pop_front();
-        S->queue_tk.pop_front();
+        qr.pop_front();
+        qt.pop_front();
     }
     if (B.tickets.empty()) {   // nothing admitted: let go of the chunks pinned while trying
         for (ChunkRes *c : B.pins) unpin_chunk(S, c);
         B.pins.clear();
+        B.waits.clear();
         S->pending_upd.swap(B.upd);   // the device tables still need these writes
         B.upd.clear();
     }
@@ -397,7 +438,11 @@ void CUDART_CB on_done(void *p) {
 // Enqueues a formed batch on the stream: misses into their slots, gather,
 // host copies, completion callback.
 bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
-    cudaStream_t s = L.stream;
+    cudaStream_t s = S->stream[B.cls];
+    // after the archive mirror's sync and the other class's decodes it reads
+    if (!cuda_ok(cudaStreamWaitEvent(s, S->mirror_ev, 0), "stream wait")) return false;
+    for (cudaEvent_t e : B.waits)
+        if (!cuda_ok(cudaStreamWaitEvent(s, e, 0), "stream wait")) return false;
     const size_t nu = B.upd.size();
     if (nu) {
         if (!B.h_upd.ensure(sizeof(uint2) * nu) || !B.d_upd.ensure(sizeof(uint2) * nu)) return false;
@@ -412,6 +457,7 @@ bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
         memcpy(B.dec.h_items.p, B.miss.data(), sizeof(DecItem) * nmiss);
         if (!decode_prepare_staged(B.dec, nmiss, s) || !decode_enqueue(B.dec, L.cfg, s)) return false;
     }
+    if (!cuda_ok(cudaEventRecord(B.decoded, s), "event record")) return false;
     if (!S->dev_out) {   // host outputs: destinations were offsets into the staging buffer
         if (!B.staging.ensure(std::max<size_t>(B.staged, 256))) return false;
         for (auto &g : B.gather) g.dst += (uint64_t)(uintptr_t)B.staging.p;
@@ -441,7 +487,18 @@ void retire(mc_b200_server *S, SrvBatch &B) {   // caller holds the lock
     B.pins.clear();
     B.busy = false;
     B.gpu_done = false;
-    S->head_blocked = false;
+    for (int c = 0; c < kClasses; ++c) S->head_blocked[c] = false;
+    S->cv_done.notify_all();
+}
+
+void fail_queued(mc_b200_server *S) {   // caller holds the lock
+    for (int c = 0; c < kClasses; ++c) {
+        while (!S->queue_tk[c].empty()) {
+            S->tickets[S->queue_tk[c].front()].state = -1;
+            S->queue_tk[c].pop_front();
+            S->queue_req[c].pop_front();
+        }
+    }
     S->cv_done.notify_all();
 }
 
@@ -450,40 +507,54 @@ void worker_main(mc_b200_server *S) {
     std::unique_lock<std::mutex> lk(S->mu);
     if (!L) {   // no usable device: refuse everything
         S->stop = true;
-        while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-        S->cv_done.notify_all();
+        fail_queued(S);
         return;
     }
+    // a class whose queue is waiting and one of whose batches is free; the
+    // small class first
+    auto ready_class = [&]() -> int {
+        for (int c = 0; c < kClasses; ++c) {
+            if (S->queue_req[c].empty() || S->head_blocked[c]) continue;
+            for (auto &b : S->batch[c])
+                if (!b.busy) return c;
+        }
+        return -1;
+    };
     for (;;) {
+        S->waiting = true;
         S->cv.wait(lk, [&] {
-            bool any_busy = false, any_free = false;
-            for (auto &b : S->batch) {
-                if (b.busy && b.gpu_done) return true;
-                any_busy |= b.busy;
-                any_free |= !b.busy;
-            }
-            if (!S->queue_req.empty() && any_free && !S->head_blocked) return true;
-            return S->stop && S->queue_req.empty() && !any_busy;
+            bool any_busy = false;
+            for (auto &cb : S->batch)
+                for (auto &b : cb) {
+                    if (b.busy && b.gpu_done) return true;
+                    any_busy |= b.busy;
+                }
+            if (ready_class() >= 0) return true;
+            return S->stop && queues_empty(S) && !any_busy;
         });
-        for (auto &b : S->batch)
-            if (b.busy && b.gpu_done) retire(S, b);
-        if (S->stop && S->queue_req.empty()) {   // closing: drain what is in flight, then leave
+        S->waiting = false;
+        for (auto &cb : S->batch)
+            for (auto &b : cb)
+                if (b.busy && b.gpu_done) retire(S, b);
+        if (S->stop && queues_empty(S)) {   // closing: drain what is in flight, then leave
             bool busy = false;
-            for (auto &b : S->batch) busy |= b.busy;
+            for (auto &cb : S->batch)
+                for (auto &b : cb) busy |= b.busy;
             if (!busy) break;
             continue;
         }
+        const int cls = ready_class();
+        if (cls < 0) continue;
         SrvBatch *fb = nullptr;
-        for (auto &b : S->batch)
+        for (auto &b : S->batch[cls])
             if (!b.busy) { fb = &b; break; }
-        if (!fb || S->queue_req.empty()) continue;
         // the archive mirror up to date, ordered before this batch's work
         lk.unlock();
         const uint8_t *dbase = mirror_sync(S->a, *L);
+        const bool synced = dbase && cuda_ok(cudaEventRecord(S->mirror_ev, L->stream), "event record");
         lk.lock();
-        if (!dbase) {
-            while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-            S->cv_done.notify_all();
+        if (!synced) {
+            fail_queued(S);
             continue;
         }
         form(S, *fb, dbase);
@@ -494,18 +565,32 @@ void worker_main(mc_b200_server *S) {
         const bool ok = launch(S, *fb, *L);
         lk.lock();
         if (!ok) {
-            cudaStreamSynchronize(L->stream);
+            cudaStreamSynchronize(S->stream[fb->cls]);
             for (long t : fb->tickets) S->tickets[t].state = -1;
             fb->gpu_done = true;
             retire(S, *fb);
         }
     }
-    // fail whatever is still queued
-    while (!S->queue_tk.empty()) { S->tickets[S->queue_tk.front()].state = -1; S->queue_tk.pop_front(); S->queue_req.pop_front(); }
-    S->cv_done.notify_all();
+    fail_queued(S);   // whatever is still queued
 }
 
 }  // namespace
+
+// Frees a server whose worker is not running (never started or joined).
+static void server_free(mc_b200_server *S) {
+    for (int c = 0; c < kClasses; ++c)
+        if (S->stream[c]) cudaStreamSynchronize(S->stream[c]);
+    if (S->d_cache) cudaFree(S->d_cache);
+    if (S->d_tables) cudaFree(S->d_tables);
+    for (int c = 0; c < kClasses; ++c) {
+        for (auto &b : S->batch[c])
+            if (b.decoded) cudaEventDestroy(b.decoded);
+        if (S->stream[c]) cudaStreamDestroy(S->stream[c]);
+    }
+    if (S->mirror_ev) cudaEventDestroy(S->mirror_ev);
+    for (auto &kv : S->chunks) delete kv.second;
+    delete S;
+}
 
 extern "C" {
 
@@ -518,18 +603,32 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
     S->dev_out = out_on_device != 0;
     S->batch_bytes = batch_bytes ? batch_bytes : ((size_t)256 << 20);
     S->nslots = (uint32_t)std::min<size_t>(cache_bytes / kN3, 0xFFFFFFF0u);
-    if (!cuda_ok(cudaMalloc(&S->d_cache, (size_t)S->nslots * kN3), "cache alloc")) { delete S; return nullptr; }
+    if (!cuda_ok(cudaMalloc(&S->d_cache, (size_t)S->nslots * kN3), "cache alloc")) { server_free(S); return nullptr; }
     S->slot_owner.assign(S->nslots, nullptr);
     S->slot_block.assign(S->nslots, 0);
     // slot tables: room for every chunk the cache could hold a block of, within reason
     S->ntables = (uint32_t)std::min<size_t>(std::max<size_t>(S->nslots, 1024), 16384);
     if (!cuda_ok(cudaMalloc(&S->d_tables, (size_t)S->ntables * kGrid3 * 4), "table alloc")) {
-        cudaFree(S->d_cache);
-        delete S;
+        server_free(S);
         return nullptr;
     }
     S->table_owner.assign(S->ntables, nullptr);
     for (uint32_t t = S->ntables; t-- > 0;) S->free_tables.push_back(t);
+    // the small class on the device's highest stream priority (numerically least)
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    bool ok = cuda_ok(cudaStreamCreateWithPriority(&S->stream[0], cudaStreamNonBlocking, prio_hi), "stream") &&
+              cuda_ok(cudaStreamCreateWithPriority(&S->stream[1], cudaStreamNonBlocking, prio_lo), "stream") &&
+              cuda_ok(cudaEventCreateWithFlags(&S->mirror_ev, cudaEventDisableTiming), "event");
+    for (int c = 0; c < kClasses && ok; ++c)
+        for (auto &b : S->batch[c]) {
+            b.cls = c;
+            ok = ok && cuda_ok(cudaEventCreateWithFlags(&b.decoded, cudaEventDisableTiming), "event");
+        }
+    if (!ok) {
+        server_free(S);
+        return nullptr;
+    }
     S->worker = std::thread(worker_main, S);
     return S;
 }
@@ -548,9 +647,10 @@ long mc_b200_server_submit(mc_b200_server *S, const mc_b200_request *r) {
     const long t = (long)S->tickets.size();
     S->tickets.emplace_back();
     S->tickets.back().t_submit = now_ns();
-    S->queue_req.push_back(*r);
-    S->queue_tk.push_back(t);
-    S->cv.notify_one();
+    const int c = class_of(*r);
+    S->queue_req[c].push_back(*r);
+    S->queue_tk[c].push_back(t);
+    if (S->waiting) S->cv.notify_one();
     return t;
 }
 
@@ -618,11 +718,7 @@ void mc_b200_server_close(mc_b200_server *S) {
         S->cv.notify_one();
     }
     if (S->worker.joinable()) S->worker.join();
-    cudaDeviceSynchronize();
-    if (S->d_cache) cudaFree(S->d_cache);
-    if (S->d_tables) cudaFree(S->d_tables);
-    for (auto &kv : S->chunks) delete kv.second;
-    delete S;
+    server_free(S);
 }
 
 }  // extern "C"

@@ -1,6 +1,7 @@
 """The serving loop (mc_b200_server): block, region and chunk requests batched
 behind the HBM decoded-block cache must return exactly what the plain per-call
-reads return -- alone, in a mix, after evictions, and for host outputs."""
+reads return -- alone, in a mix, after evictions, and for host outputs -- and
+what the oracle decodes from the archive file's own blobs."""
 import numpy as np
 import pytest
 
@@ -33,6 +34,7 @@ def archive(gpu, tmp_path_factory):
     l1 = [volumes.region(12, (0, 0, 256 * i), (256, 256, 256), 0.3, device="cuda").contiguous() for i in range(2)]
     assert a.append_chunks(1, [(0, 0, 0), (0, 0, 1)], [v.data_ptr() for v in l1], 3.0, on_device=True) == 0
     torch.cuda.synchronize()
+    a.path = path
     yield a
     a.close()
 
@@ -149,3 +151,69 @@ def test_replay_trace(archive):
     assert st["batches"] > 1
     for i in range(0, len(reqs), 17):
         assert np.array_equal(outs[i].cpu().numpy(), expected(archive, reqs[i])), reqs[i]
+
+
+def _oracle_volume(oracle, arch, lod, cz, cy, cx, cache):
+    """Chunk (lod, cz, cy, cx) decoded by the oracle from the archive file's own
+    blob bytes (zeros for an absent or all-air chunk)."""
+    import shapes
+    key = (lod, cz, cy, cx)
+    if key not in cache:
+        data = cache.setdefault("data", open(arch.path, "rb").read())
+        co = arch.chunk_offset(lod, cz, cy, cx)
+        if co <= 1:
+            cache[key] = np.zeros((256, 256, 256), np.uint8)
+        else:
+            cache[key] = oracle.decode_chunk(data[co:co + shapes.blob_len(data, co)]).reshape(256, 256, 256)
+    return cache[key]
+
+
+def _oracle_expected(oracle, arch, r, cache):
+    kind, lod, z, y, x, dz, dy, dx = r
+    if kind == REQ_BLOCK:
+        v = _oracle_volume(oracle, arch, lod, z >> 4, y >> 4, x >> 4, cache)
+        bz, by, bx = z & 15, y & 15, x & 15
+        return v[bz * 16:bz * 16 + 16, by * 16:by * 16 + 16, bx * 16:bx * 16 + 16].reshape(-1)
+    if kind == REQ_CHUNK:
+        return _oracle_volume(oracle, arch, lod, z, y, x, cache).reshape(-1)
+    out = np.zeros((dz, dy, dx), np.uint8)
+    for cz in range(z >> 8, ((z + dz - 1) >> 8) + 1):
+        for cy in range(y >> 8, ((y + dy - 1) >> 8) + 1):
+            for cx in range(x >> 8, ((x + dx - 1) >> 8) + 1):
+                if min(cz, cy, cx) < 0 or max(cz, cy, cx) > 1:
+                    continue   # outside the volume: zeros
+                v = _oracle_volume(oracle, arch, lod, cz, cy, cx, cache)
+                zs, ze = max(z, cz * 256), min(z + dz, cz * 256 + 256)
+                ys, ye = max(y, cy * 256), min(y + dy, cy * 256 + 256)
+                xs, xe = max(x, cx * 256), min(x + dx, cx * 256 + 256)
+                if zs < ze and ys < ye and xs < xe:
+                    out[zs - z:ze - z, ys - y:ye - y, xs - x:xe - x] = \
+                        v[zs - cz * 256:ze - cz * 256, ys - cy * 256:ye - cy * 256, xs - cx * 256:xe - cx * 256]
+    return out.reshape(-1)
+
+
+def test_served_matches_oracle(archive, oracle):
+    """Served results against the oracle's own decode of the archive file's
+    blobs (not the library's per-call paths): blocks, regions across chunk
+    borders and past the volume, chunks, absent and all-air chunks."""
+    rng = np.random.default_rng(10)
+    reqs = [r for r in mixed_requests(rng, 60) if r[1] == 0]
+    with Server(archive, 256 << 20, 64 << 20) as srv:
+        got = run(srv, reqs)
+    cache = {}
+    for r, g in zip(reqs, got):
+        assert np.array_equal(g, _oracle_expected(oracle, archive, r, cache)), r
+
+
+def test_small_class_reads_large_class_misses(archive):
+    """A chunk request (large class) whose blocks are all misses, then block
+    requests (small class, another stream) inside that chunk submitted right
+    behind it: the block batches find the blocks already assigned to cache
+    slots and must wait for the chunk batch's decode before they gather."""
+    for trial in range(3):
+        reqs = [(REQ_CHUNK, 0, 1, 0, 1, 0, 0, 0)] + \
+               [(REQ_BLOCK, 0, 16 + (5 * i) % 16, 3 + i, 16 + (7 * i) % 16, 0, 0, 0) for i in range(12)]
+        with Server(archive, 256 << 20, 64 << 20) as srv:
+            got = run(srv, reqs)
+        for r, g in zip(reqs, got):
+            assert np.array_equal(g, expected(archive, r)), (trial, r)
