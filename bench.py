@@ -296,27 +296,16 @@ def run_serve(args):
                                             for k in range(3) if (tr.kind == k).any()},
                          "hit_rate": round(st["hits"] / max(1, st["hits"] + st["misses"]), 4),
                          "batches": st["batches"]})
-    # plain per-call drop-in: the same mix, one call at a time, host outputs
+    # plain per-call drop-in on the same mix, one call at a time: with device
+    # outputs (like for like with the server's device outputs) and with host
+    # outputs (the reference's own call signatures)
     tr = workloads.Trace(99, 400, 1e4, VOLUME_DIMS, lods=4)
-    lat, nbytes = [], 0
-    host = [np.empty(n, np.uint8) for n in (4096, 128 ** 3, 256 ** 3)]
-    t_all = time.perf_counter()
-    for i in range(len(tr)):
-        k, lod = int(tr.kind[i]), int(tr.lod[i])
-        z, y, x, dz, dy, dx = (int(v) for v in tr.req[i, :6])
-        t1 = time.perf_counter()
-        if k == 0:
-            co = a.chunk_offset(lod, z >> 4, y >> 4, x >> 4)
-            if co > 1:
-                a.decode_block(co, z & 15, y & 15, x & 15)
-        elif k == 1:
-            a.read_region(lod, z, y, x, dz, dy, dx, out=host[1])
-        else:
-            a.decode_chunk(a.chunk_offset(lod, z, y, x), out=host[2])
-        lat.append((time.perf_counter() - t1) * 1e3)
-        nbytes += tr.out_bytes(i)
-    plain_s = time.perf_counter() - t_all
+    plain_dev = plain_per_call(a, tr, outs, device=True)
+    plain_host = plain_per_call(a, tr, None, device=False)
     a.close()
+    # the reference's decoded-block cache (mc_cache_new_archive, 8 GiB) on the
+    # same 400 requests, one at a time on the host
+    ref_cache = reference_cache_trace(path, tr, args.q)
     os.remove(path)
     os.rmdir(td)
     return {"metric": "serving: p50/p99 request latency and GB/s of a Poisson block/region/chunk mix",
@@ -325,12 +314,91 @@ def run_serve(args):
                                    f"LOD 0-3, q={args.q:g}, {nch} chunks",
                        "mix": "70% 16^3 blocks, 20% 128^3 regions, 10% 256^3 chunks",
                        "locality": "Zipf(1.1) over 128^3 cells", "cache": "8 GiB HBM decoded-block cache, FIFO",
+                       "classes": "requests up to 256 KiB of output batched on a high-priority stream, larger ones "
+                                  "on a normal stream",
                        "outputs": "device memory", "batch_bytes": 512 << 20,
                        "archive_build_s": round(build_s, 2)},
             "rates": rows,
-            "plain_per_call": {"api": "mc_archive_decode_block / read_region / decode_chunk (host outputs)",
-                               "requests": len(tr), "p50_ms": round(pct(lat, 50), 4), "p99_ms": round(pct(lat, 99), 4),
-                               "gbs": round(nbytes / plain_s / 1e9, 3)}}
+            "plain_per_call_device": plain_dev, "plain_per_call_host": plain_host,
+            "reference_cache": ref_cache}
+
+
+NAMES = ("block", "region", "chunk")
+
+
+def _lat_summary(tr, lat, nbytes, seconds, api):
+    lat = np.asarray(lat, np.float64)
+    return {"api": api, "requests": len(tr), "p50_ms": round(pct(lat, 50), 4), "p99_ms": round(pct(lat, 99), 4),
+            "p99_ms_by_kind": {NAMES[k]: round(pct(lat[tr.kind == k], 99), 4) for k in range(3) if (tr.kind == k).any()},
+            "gbs": round(nbytes / seconds / 1e9, 3)}
+
+
+def plain_per_call(a, tr, outs, device):
+    """The trace's requests one call at a time through the plain entry points:
+    device outputs (mc_b200_read_regions_dev for blocks and regions,
+    mc_b200_decode_chunks_dev for chunks; each call waits for its result) or
+    host outputs (mc_archive_decode_block / read_region / decode_chunk)."""
+    host = [np.empty(n, np.uint8) for n in (4096, 128 ** 3, 256 ** 3)]
+    lat, nbytes = [], 0
+    t_all = time.perf_counter()
+    for i in range(len(tr)):
+        k, lod = int(tr.kind[i]), int(tr.lod[i])
+        z, y, x, dz, dy, dx = (int(v) for v in tr.req[i, :6])
+        t1 = time.perf_counter()
+        if device:
+            if k == 0:
+                a.read_regions_dev(lod, [(z * 16, y * 16, x * 16)], 16, 16, 16, outs[0].data_ptr())
+            elif k == 1:
+                a.read_regions_dev(lod, [(z, y, x)], dz, dy, dx, outs[1].data_ptr())
+            else:
+                a.decode_chunks_dev([a.chunk_offset(lod, z, y, x)], outs[2].data_ptr())
+        else:
+            if k == 0:
+                co = a.chunk_offset(lod, z >> 4, y >> 4, x >> 4)
+                if co > 1:
+                    a.decode_block(co, z & 15, y & 15, x & 15)
+            elif k == 1:
+                a.read_region(lod, z, y, x, dz, dy, dx, out=host[1])
+            else:
+                a.decode_chunk(a.chunk_offset(lod, z, y, x), out=host[2])
+        lat.append((time.perf_counter() - t1) * 1e3)
+        nbytes += tr.out_bytes(i)
+    secs = time.perf_counter() - t_all
+    api = ("mc_b200_read_regions_dev / mc_b200_decode_chunks_dev (device outputs)" if device else
+           "mc_archive_decode_block / read_region / decode_chunk (host outputs)")
+    return _lat_summary(tr, lat, nbytes, secs, api)
+
+
+def reference_cache_trace(path, tr, q):
+    """The reference's own mc_cache (8 GiB, bound to the archive) serving the
+    trace one request at a time on the host (oracle/mc_cache_trace.c over the
+    reference's default-flag build)."""
+    from oracle import HERE as ORACLE_DIR
+    lib_path = os.path.join(ORACLE_DIR, "_ref", "libmccachetrace.so")
+    if not os.path.exists(lib_path):
+        return {"unavailable": "oracle/_ref/libmccachetrace.so not built"}
+    L = C.CDLL(lib_path)
+    L.mcct_run.restype = C.c_int
+    L.mcct_run.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_size_t, C.c_int, C.c_int,
+                           C.c_void_p, C.c_void_p, C.c_void_p]
+    n = len(tr)
+    req = np.zeros((n, 8), np.int64)
+    req[:, 0] = tr.kind
+    req[:, 1] = tr.lod
+    req[:, 2:8] = tr.req[:, :6]
+    out = np.empty(256 ** 3, np.uint8)
+    lat = np.zeros(n, np.float64)
+    nz, ny, nx = VOLUME_DIMS
+    t0 = time.perf_counter()
+    rc = L.mcct_run(path.encode(), nx, ny, nz, q, 8 << 30, 0, n, req.ctypes.data, out.ctypes.data, lat.ctypes.data)
+    secs = time.perf_counter() - t0
+    if rc != 0:
+        return {"unavailable": "mcct_run failed"}
+    nbytes = sum(tr.out_bytes(i) for i in range(n))
+    r = _lat_summary(tr, lat, nbytes, secs, "reference mc_cache_new_archive(8 GiB) + mc_cache_update / "
+                                             "mc_cache_get_copy, one request at a time, host cores")
+    r["cores"] = min(os.cpu_count() or 4, 16)
+    return r
 
 
 def run_regions(args):
