@@ -6,7 +6,7 @@
 // coordinates, and the output address of chunk-local voxel (0,0,0). Every
 // resident chunk owns a table of 4096 cache-slot numbers in device memory;
 // kZeroSlot marks an absent (all-air) block. The gather flattens all items'
-// blocks into one index space and copies one block per warp.
+// blocks into one index space; each warp copies one contiguous run of it.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -26,16 +26,34 @@ __global__ void __launch_bounds__(256) k_table_update(const uint2 *upd, int n, u
 __global__ void __launch_bounds__(128) k_gather_boxes(const GatherItem *items, int nitems, uint32_t nblocks,
                                                       const uint32_t *tables, const uint8_t *cache) {
     const int lane = threadIdx.x & 31;
+    // each warp copies one contiguous run of flattened blocks: x-adjacent
+    // blocks of an item follow each other, so the 16-byte row pieces of
+    // neighbouring blocks reach L2 close together and fill whole sectors, and
+    // the item holding a block is found by one search per warp, then by
+    // stepping forward
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nblocks; g += nwarps) {
-        // the item holding flattened block g: the last one whose first <= g
+    const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t per = (nblocks + nwarps - 1) / nwarps;
+    const uint32_t g0 = w * per, g1 = min(nblocks, g0 + per);
+    if (g0 >= g1) return;
+    int cur;
+    {   // the last item whose first <= g0
         int lo = 0, hi = nitems - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].first <= g) lo = mid;
+            if (items[mid].first <= g0) lo = mid;
             else hi = mid - 1;
         }
-        const GatherItem it = items[lo];
+        cur = lo;
+    }
+    GatherItem it = items[cur];
+    uint32_t next_first = cur + 1 < nitems ? items[cur + 1].first : 0xFFFFFFFFu;
+    for (uint32_t g = g0; g < g1; ++g) {
+        while (g >= next_first) {
+            ++cur;
+            it = items[cur];
+            next_first = cur + 1 < nitems ? items[cur + 1].first : 0xFFFFFFFFu;
+        }
         const uint32_t local = g - it.first;
         const int bz0 = it.box_lo >> 8, by0 = (it.box_lo >> 4) & 15, bx0 = it.box_lo & 15;
         const int nby = ((it.box_hi >> 4) & 15) - by0 + 1, nbx = (it.box_hi & 15) - bx0 + 1;
@@ -79,9 +97,11 @@ cudaError_t launch_table_update(const uint2 *d_upd, int n, uint32_t *d_tables, c
 cudaError_t launch_gather_boxes(const GatherItem *d_items, int nitems, uint32_t nblocks, const uint32_t *d_tables,
                                 const uint8_t *d_cache, cudaStream_t s) {
     if (nitems <= 0 || nblocks == 0) return cudaSuccess;
-    uint32_t blocks = (nblocks + 3) / 4;
+    // at least 8 blocks per warp where the batch allows; at most 8 CTAs per SM
+    uint32_t blocks = (nblocks + 31) / 32;
     const uint32_t cap = (uint32_t)sm_count() * 8;
     if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
     k_gather_boxes<<<blocks, 128, 0, s>>>(d_items, nitems, nblocks, d_tables, d_cache);
     return cudaGetLastError();
 }
