@@ -347,10 +347,10 @@ __device__ __forceinline__ void slow_work(LaneState &L, const EntParams &P, cons
     L.st = S_DONE;
 }
 
-// Predicated global store (one instruction, no branch).
+// Predicated global store (the compiler turns this into one predicated
+// instruction, no branch).
 __device__ __forceinline__ void stg_if(bool pred, uint32_t *p, uint32_t v) {
-    asm volatile("{.reg .pred q; setp.ne.u32 q, %2, 0; @q st.global.u32 [%0], %1;}"
-                 :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
+    if (pred) *p = v;
 }
 
 // The rare events of a fast step, in this order: a window refill, the rest of

@@ -45,9 +45,6 @@ static uint32_t BYTE_PERM(uint32_t x, uint32_t y, uint32_t s) {
 namespace mcb {
 '''
 
-_STORES = r'''static inline void stg_if(bool pred, uint32_t *p, uint32_t v) { if (pred) *p = v; }
-
-'''
 
 _DRIVER = r'''
 #include <vector>
@@ -119,8 +116,6 @@ def _host_source():
     src = open(os.path.join(CSRC, "mcb_decode.cu")).read()
     stage1 = _cut(src, "// ---------------------------------------------------------------- stage 1",
                   "template <int WARPS>\n__global__")
-    stores = _cut(stage1, "// Predicated global store", "// The rare events of a fast step")
-    stage1 = stage1.replace(stores, _STORES)
     solo = _cut(src, "// The whole stream of one block on one lane", "static_assert(sizeof(DecItem)")
     body = stage1 + solo
     for dev, host in (("__device__ __forceinline__", "static inline"), ("__ldg(", "LDG("),
