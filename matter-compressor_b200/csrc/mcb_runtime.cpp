@@ -160,7 +160,11 @@ Lane *lane() {
 }
 
 // ------------------------------------------------------------------ decode
-static constexpr uint64_t kArenaMaxEntries = 256ull << 20;   // 1 GiB of entries per sub-batch
+// 8 GiB of entries per sub-batch: the per-block bound is 8 entries per payload
+// byte, so a 64-chunk batch at q = 1 (about 1 KB per block) needs 6 GiB; a
+// split would run the entropy stage once per sub-batch, each run bounded by
+// its longest block's serial chain.
+static constexpr uint64_t kArenaMaxEntries = 2048ull << 20;
 static constexpr uint32_t kPoolEntries = 4u << 20;           // overflow pool, 16 MiB
 
 // Splits the items into sub-batches that fit the arena, writes each item's

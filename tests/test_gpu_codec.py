@@ -304,7 +304,8 @@ def test_plan_entropy_shapes(gpu, oracle, tmp_path):
                 plan.launch()
                 torch.cuda.synchronize()
                 assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim)
-            assert plan.set_tuning(3, 4, 1, 4, "sequential") == -1   # 3 warps per CTA: refused
+            with pytest.raises(RuntimeError, match="bad arguments"):   # 3 warps per CTA: refused
+                plan.set_tuning(3, 4, 1, 4, "sequential")
         finally:
             plan.free()
 
