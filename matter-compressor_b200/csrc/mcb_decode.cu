@@ -682,14 +682,6 @@ constexpr int kStageBytes = 16 * kStageZ;
 // every block puts them back).
 __shared__ int s_rec_ext[3];
 __shared__ float s_rec_l1;
-// Per-plane and per-line-group extents of the same block: s_rec_ymax[cz] is one
-// past the largest cy of a coefficient in plane cz (0: empty plane), and
-// s_rec_xmax[cz*4 + g] one past the largest cx in lines cy = 4g..4g+3 of it.
-// The x and y passes run over these, not over the block's box: the lines and
-// terms they leave out hold only zero coefficients, which the reference skips
-// too (src/mc_codec_float.h:98-105, 119-126).
-__shared__ int s_rec_ymax[16];
-__shared__ int s_rec_xmax[64];
 
 // Before a CTA's first block: an all-zero coefficient box, zero extents and
 // L1 norm. The caller synchronises before the first block.
@@ -698,8 +690,6 @@ __device__ __forceinline__ void rec_init(float *sB) {
         reinterpret_cast<float4 *>(sB)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (threadIdx.x < 3) s_rec_ext[threadIdx.x] = 0;
     if (threadIdx.x == 3) s_rec_l1 = 0.0f;
-    if (threadIdx.x < 16) s_rec_ymax[threadIdx.x] = 0;
-    if (threadIdx.x < 64) s_rec_xmax[threadIdx.x] = 0;
 }
 
 // Reconstruct one block into a stage (z slices of kStageZ bytes). Thread t owns the
@@ -767,8 +757,6 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
                 mz = max(mz, cz);
                 my = max(my, cy);
                 mx = max(mx, cx);
-                atomicMax(&s_rec_ymax[cz], cy + 1);
-                atomicMax(&s_rec_xmax[cz * 4 + (cy >> 2)], cx + 1);
                 const int lv = (int16_t)(e[k] >> 16);
                 if (lv) {
                     const int f = cz + cy + cx;
@@ -793,14 +781,13 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         }
         __syncthreads();
         E = s_rec_ext[0] + 1;
-        const int Y = s_rec_ext[1] + 1;   // plane stride of the pass-1 output
+        const int Y = s_rec_ext[1] + 1, X = s_rec_ext[2] + 1;
         const bool fast = s_rec_l1 < kFastL1;
         if ((uint32_t)tid < nlines)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(P.arena + nbase + 32ull * tid));
         // pass 1: lines along x for 4 adjacent cy at once, box[cz][k][cy..cy+3]
-        // -> A[cz*Y + cy][x]. Group g of plane cz holds lines cy = 4g..4g+3 and
-        // sums its s_rec_xmax terms; lines at or past the plane's s_rec_ymax
-        // are not stored (pass 2 does not read them). gi < 64, so
+        // -> A[cz*Y + cy][x]. Group g of plane cz holds lines cy = 4g..4g+3;
+        // lines at cy >= Y are zero and not stored. gi < 64, so
         // gi * ceil(2^16 / G) >> 16 is exactly gi / G.
         const int mh = tid & 3;   // this thread's output pair (m, m+1) = (2mh, 2mh+1)
         const int G = (Y + 3) >> 2;
@@ -809,17 +796,14 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
             const int gi = t >> 2;
             const int cz = (gi * invG) >> 16;
             const int cy0 = (gi - cz * G) << 2;
-            const int ycz = s_rec_ymax[cz];
-            if (cy0 >= ycz) continue;
-            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + cz * kBoxPlane + cy0), 4,
-                                  s_rec_xmax[cz * 4 + (cy0 >> 2)], W, mh);
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sB + cz * kBoxPlane + cy0), 4, X, W, mh);
             // line i of the group: outputs m, m+1 (e + o) and 15-m, 14-m (e - o)
             const float2 p0 = add2(a.e0a, a.o0a), p1 = add2(a.e0b, a.o0b);
             const float2 q0 = add2(a.e1a, a.o1a), q1 = add2(a.e1b, a.o1b);
             const float2 r0 = sub2(a.e0a, a.o0a), r1 = sub2(a.e0b, a.o0b);
             const float2 s0 = sub2(a.e1a, a.o1a), s1 = sub2(a.e1b, a.o1b);
             float *out = sA + (cz * Y + cy0) * kRowF;
-            const int nl = min(ycz - cy0, 4);
+            const int nl = min(Y - cy0, 4);
             *reinterpret_cast<float2 *>(out + m) = make_float2(p0.x, q0.x);
             *reinterpret_cast<float2 *>(out + 14 - m) = make_float2(s0.x, r0.x);
             if (nl > 1) {
@@ -842,8 +826,8 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         // pass 2: lines along y for 4 adjacent x at once, A[cz][k][x..x+3] -> B[cz][y][x..x+3]
         for (int t = tid; t < E * 16; t += 128) {
             const int xg = (t >> 2) & 3, cz = t >> 4;
-            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sA + cz * Y * kRowF + xg * 4), kRowF / 4,
-                                  s_rec_ymax[cz], W, mh);
+            const Acc4 a = lines4(reinterpret_cast<const float4 *>(sA + cz * Y * kRowF + xg * 4), kRowF / 4, Y,
+                                  W, mh);
             // rows m, m+1 swizzle by bswz(m) = mh, rows 15-m, 14-m by 3 - mh
             float *ob = sB + cz * kPlaneB;
             const int ga = (xg ^ mh) << 2, gb = (xg ^ (3 - mh)) << 2;
@@ -878,12 +862,9 @@ __device__ __forceinline__ void reconstruct_block(const RecParams &P, int item, 
         }
     }
     __syncthreads();
-    // the box planes this block wrote (coefficients and pass-2 output) and the
-    // per-plane extents back to zero
+    // the box planes this block wrote (coefficients and pass-2 output) back to zero
     for (int i = tid; i < E * (kBoxPlane / 4); i += 128)
         reinterpret_cast<float4 *>(sB)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (tid < 16) s_rec_ymax[tid] = 0;
-    if (tid < 64) s_rec_xmax[tid] = 0;
     if (ncorr && tid == 0) {
         // corrections in stream order: a position may repeat, each
         // application clamps (src/mc_codec.c:775-781)
