@@ -494,7 +494,14 @@ __device__ __forceinline__ void run_lanes(LaneState &L, const EntParams &P, uint
     L.st = S_DONE;
     Claim c{gtid, gtid + 1};
     for (;;) {
-        while (!__any_sync(0xFFFFFFFFu, L.st >= S_END)) fast_step(L, P, ctx, s_bend);
+        // two steps per loop turn (the loop-carried lane state then needs
+        // no register shuffling between the two), the check after each
+        for (;;) {
+            if (__any_sync(0xFFFFFFFFu, L.st >= S_END)) break;
+            fast_step(L, P, ctx, s_bend);
+            if (__any_sync(0xFFFFFFFFu, L.st >= S_END)) break;
+            fast_step(L, P, ctx, s_bend);
+        }
         while (L.st >= S_END) {
             if (L.st != S_DONE) {
                 slow_work(L, P, ctx, s_bend);
