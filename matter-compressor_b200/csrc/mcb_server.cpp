@@ -17,8 +17,8 @@
 //             cache into its output (one launch), and marks the tickets done
 //             from a stream callback.
 //
-// Requests travel in two classes, each with its own queue, its own CUDA
-// stream and two batches in flight at most: small requests (a block, a small
+// Requests travel in two classes, each with its own queue, its own worker
+// thread, its own CUDA stream and two batches in flight at most: small requests (a block, a small
 // region) on a high-priority stream, large ones (regions over 256 KiB of
 // output, chunks) on a normal one. A block request therefore never waits
 // behind a chunk's decode in the same batch, and the GPU runs a small batch's
@@ -128,19 +128,19 @@ struct mc_b200_server {
     std::vector<uint2> pending_upd;   // table writes of a formed batch that admitted nothing
     // requests
     std::mutex mu;
-    std::condition_variable cv;        // the worker: new requests, finished batches, close
+    std::condition_variable cv[kClasses];   // a class's worker: new requests, finished batches, close
     std::condition_variable cv_done;   // callers waiting for tickets
     std::deque<mc_b200_request> queue_req[kClasses];
     std::deque<long> queue_tk[kClasses];
     std::deque<Ticket> tickets;
     SrvBatch batch[kClasses][kBatchesPerClass];
     cudaStream_t stream[kClasses] = {nullptr, nullptr};
-    cudaEvent_t mirror_ev = nullptr;   // the archive mirror's last sync on the worker's lane stream
+    cudaEvent_t mirror_ev[kClasses] = {nullptr, nullptr};   // each worker's last mirror sync on its lane stream
     uint64_t seq = 0;
     bool stop = false;
-    bool waiting = false;              // the worker sleeps on cv
+    bool waiting[kClasses] = {false, false};        // a worker sleeps on its cv
     bool head_blocked[kClasses] = {false, false};   // a queue head waits for cache slots held by a batch in flight
-    std::thread worker;
+    std::thread worker[kClasses];
     // statistics
     uint64_t st_req = 0, st_batches = 0, st_blocks = 0, st_hits = 0, st_miss = 0, st_zero = 0, st_evict = 0,
              st_bytes = 0;
@@ -157,12 +157,6 @@ size_t out_bytes(const mc_b200_request &r) {
 }
 
 int class_of(const mc_b200_request &r) { return out_bytes(r) <= kSmallBytes ? 0 : 1; }
-
-bool queues_empty(const mc_b200_server *S) {
-    for (int c = 0; c < kClasses; ++c)
-        if (!S->queue_req[c].empty()) return false;
-    return true;
-}
 
 // One chunk's share of a request, before cache resolution.
 struct Piece {
@@ -432,7 +426,7 @@ void CUDART_CB on_done(void *p) {
     std::lock_guard<std::mutex> g(B->srv->mu);
     for (long k : B->tickets) B->srv->tickets[k].t_done = t;
     B->gpu_done = true;
-    B->srv->cv.notify_one();
+    B->srv->cv[B->cls].notify_one();
 }
 
 // Enqueues a formed batch on the stream: misses into their slots, gather,
@@ -440,7 +434,7 @@ void CUDART_CB on_done(void *p) {
 bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
     cudaStream_t s = S->stream[B.cls];
     // after the archive mirror's sync and the other class's decodes it reads
-    if (!cuda_ok(cudaStreamWaitEvent(s, S->mirror_ev, 0), "stream wait")) return false;
+    if (!cuda_ok(cudaStreamWaitEvent(s, S->mirror_ev[B.cls], 0), "stream wait")) return false;
     for (cudaEvent_t e : B.waits)
         if (!cuda_ok(cudaStreamWaitEvent(s, e, 0), "stream wait")) return false;
     const size_t nu = B.upd.size();
@@ -487,74 +481,68 @@ void retire(mc_b200_server *S, SrvBatch &B) {   // caller holds the lock
     B.pins.clear();
     B.busy = false;
     B.gpu_done = false;
-    for (int c = 0; c < kClasses; ++c) S->head_blocked[c] = false;
-    S->cv_done.notify_all();
-}
-
-void fail_queued(mc_b200_server *S) {   // caller holds the lock
+    // slots and tables this batch held are free again: either class may go on
     for (int c = 0; c < kClasses; ++c) {
-        while (!S->queue_tk[c].empty()) {
-            S->tickets[S->queue_tk[c].front()].state = -1;
-            S->queue_tk[c].pop_front();
-            S->queue_req[c].pop_front();
-        }
+        S->head_blocked[c] = false;
+        S->cv[c].notify_one();
     }
     S->cv_done.notify_all();
 }
 
-void worker_main(mc_b200_server *S) {
+void fail_queued(mc_b200_server *S, int c) {   // caller holds the lock
+    while (!S->queue_tk[c].empty()) {
+        S->tickets[S->queue_tk[c].front()].state = -1;
+        S->queue_tk[c].pop_front();
+        S->queue_req[c].pop_front();
+    }
+    S->cv_done.notify_all();
+}
+
+// The worker of request class c: forms its class's batches from its queue,
+// launches them on its stream and retires them. The two workers share the
+// cache bookkeeping under the server's lock; each launches without it.
+void worker_main(mc_b200_server *S, int c) {
     Lane *L = lane();
     std::unique_lock<std::mutex> lk(S->mu);
-    if (!L) {   // no usable device: refuse everything
+    if (!L) {   // no usable device: refuse everything of this class
         S->stop = true;
-        fail_queued(S);
+        fail_queued(S, c);
         return;
     }
-    // a class whose queue is waiting and one of whose batches is free; the
-    // small class first
-    auto ready_class = [&]() -> int {
-        for (int c = 0; c < kClasses; ++c) {
-            if (S->queue_req[c].empty() || S->head_blocked[c]) continue;
-            for (auto &b : S->batch[c])
-                if (!b.busy) return c;
-        }
-        return -1;
+    auto free_batch = [&]() -> SrvBatch * {
+        for (auto &b : S->batch[c])
+            if (!b.busy) return &b;
+        return nullptr;
     };
     for (;;) {
-        S->waiting = true;
-        S->cv.wait(lk, [&] {
+        S->waiting[c] = true;
+        S->cv[c].wait(lk, [&] {
             bool any_busy = false;
-            for (auto &cb : S->batch)
-                for (auto &b : cb) {
-                    if (b.busy && b.gpu_done) return true;
-                    any_busy |= b.busy;
-                }
-            if (ready_class() >= 0) return true;
-            return S->stop && queues_empty(S) && !any_busy;
+            for (auto &b : S->batch[c]) {
+                if (b.busy && b.gpu_done) return true;
+                any_busy |= b.busy;
+            }
+            if (!S->queue_req[c].empty() && !S->head_blocked[c] && free_batch()) return true;
+            return S->stop && S->queue_req[c].empty() && !any_busy;
         });
-        S->waiting = false;
-        for (auto &cb : S->batch)
-            for (auto &b : cb)
-                if (b.busy && b.gpu_done) retire(S, b);
-        if (S->stop && queues_empty(S)) {   // closing: drain what is in flight, then leave
+        S->waiting[c] = false;
+        for (auto &b : S->batch[c])
+            if (b.busy && b.gpu_done) retire(S, b);
+        if (S->stop && S->queue_req[c].empty()) {   // closing: drain what is in flight, then leave
             bool busy = false;
-            for (auto &cb : S->batch)
-                for (auto &b : cb) busy |= b.busy;
+            for (auto &b : S->batch[c]) busy |= b.busy;
             if (!busy) break;
             continue;
         }
-        const int cls = ready_class();
-        if (cls < 0) continue;
-        SrvBatch *fb = nullptr;
-        for (auto &b : S->batch[cls])
-            if (!b.busy) { fb = &b; break; }
+        SrvBatch *fb = free_batch();
+        if (!fb || S->queue_req[c].empty() || S->head_blocked[c]) continue;
         // the archive mirror up to date, ordered before this batch's work
         lk.unlock();
         const uint8_t *dbase = mirror_sync(S->a, *L);
-        const bool synced = dbase && cuda_ok(cudaEventRecord(S->mirror_ev, L->stream), "event record");
+        const bool synced = dbase && cuda_ok(cudaEventRecord(S->mirror_ev[c], L->stream), "event record");
         lk.lock();
         if (!synced) {
-            fail_queued(S);
+            fail_queued(S, c);
             continue;
         }
         form(S, *fb, dbase);
@@ -565,13 +553,13 @@ void worker_main(mc_b200_server *S) {
         const bool ok = launch(S, *fb, *L);
         lk.lock();
         if (!ok) {
-            cudaStreamSynchronize(S->stream[fb->cls]);
+            cudaStreamSynchronize(S->stream[c]);
             for (long t : fb->tickets) S->tickets[t].state = -1;
             fb->gpu_done = true;
             retire(S, *fb);
         }
     }
-    fail_queued(S);   // whatever is still queued
+    fail_queued(S, c);   // whatever is still queued
 }
 
 }  // namespace
@@ -587,7 +575,8 @@ static void server_free(mc_b200_server *S) {
             if (b.decoded) cudaEventDestroy(b.decoded);
         if (S->stream[c]) cudaStreamDestroy(S->stream[c]);
     }
-    if (S->mirror_ev) cudaEventDestroy(S->mirror_ev);
+    for (int c = 0; c < kClasses; ++c)
+        if (S->mirror_ev[c]) cudaEventDestroy(S->mirror_ev[c]);
     for (auto &kv : S->chunks) delete kv.second;
     delete S;
 }
@@ -618,8 +607,9 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     bool ok = cuda_ok(cudaStreamCreateWithPriority(&S->stream[0], cudaStreamNonBlocking, prio_hi), "stream") &&
-              cuda_ok(cudaStreamCreateWithPriority(&S->stream[1], cudaStreamNonBlocking, prio_lo), "stream") &&
-              cuda_ok(cudaEventCreateWithFlags(&S->mirror_ev, cudaEventDisableTiming), "event");
+              cuda_ok(cudaStreamCreateWithPriority(&S->stream[1], cudaStreamNonBlocking, prio_lo), "stream");
+    for (int c = 0; c < kClasses && ok; ++c)
+        ok = cuda_ok(cudaEventCreateWithFlags(&S->mirror_ev[c], cudaEventDisableTiming), "event");
     for (int c = 0; c < kClasses && ok; ++c)
         for (auto &b : S->batch[c]) {
             b.cls = c;
@@ -629,7 +619,7 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
         server_free(S);
         return nullptr;
     }
-    S->worker = std::thread(worker_main, S);
+    for (int c = 0; c < kClasses; ++c) S->worker[c] = std::thread(worker_main, S, c);
     return S;
 }
 
@@ -650,7 +640,7 @@ long mc_b200_server_submit(mc_b200_server *S, const mc_b200_request *r) {
     const int c = class_of(*r);
     S->queue_req[c].push_back(*r);
     S->queue_tk[c].push_back(t);
-    if (S->waiting) S->cv.notify_one();
+    if (S->waiting[c]) S->cv[c].notify_one();
     return t;
 }
 
@@ -715,9 +705,10 @@ void mc_b200_server_close(mc_b200_server *S) {
     {
         std::lock_guard<std::mutex> g(S->mu);
         S->stop = true;
-        S->cv.notify_one();
+        for (int c = 0; c < kClasses; ++c) S->cv[c].notify_one();
     }
-    if (S->worker.joinable()) S->worker.join();
+    for (int c = 0; c < kClasses; ++c)
+        if (S->worker[c].joinable()) S->worker[c].join();
     server_free(S);
 }
 
