@@ -302,6 +302,13 @@ def run_serve(args):
     tr = workloads.Trace(99, 400, 1e4, VOLUME_DIMS, lods=4)
     plain_dev = plain_per_call(a, tr, outs, device=True)
     plain_host = plain_per_call(a, tr, None, device=False)
+    # the plain per-call path under the same open-loop arrivals as the server:
+    # one caller thread issues each request at its arrival time (or as soon as
+    # the previous call returns), latency from arrival to return
+    plain_open = {}
+    for rate in (1000.0, 10000.0):
+        to = workloads.Trace(1000 + rates.index(rate) if rate in rates else 77, 300, rate, VOLUME_DIMS, lods=4)
+        plain_open[str(int(rate))] = plain_per_call(a, to, outs, device=True, arrivals=to.arrival_ns)
     a.close()
     # the reference's decoded-block cache (mc_cache_new_archive, 8 GiB) on the
     # same 400 requests, one at a time on the host
@@ -320,6 +327,7 @@ def run_serve(args):
                        "archive_build_s": round(build_s, 2)},
             "rates": rows,
             "plain_per_call_device": plain_dev, "plain_per_call_host": plain_host,
+            "plain_per_call_device_open_loop": plain_open,
             "reference_cache": ref_cache}
 
 
@@ -333,11 +341,14 @@ def _lat_summary(tr, lat, nbytes, seconds, api):
             "gbs": round(nbytes / seconds / 1e9, 3)}
 
 
-def plain_per_call(a, tr, outs, device):
+def plain_per_call(a, tr, outs, device, arrivals=None):
     """The trace's requests one call at a time through the plain entry points:
     device outputs (mc_b200_read_regions_dev for blocks and regions,
     mc_b200_decode_chunks_dev for chunks; each call waits for its result) or
-    host outputs (mc_archive_decode_block / read_region / decode_chunk)."""
+    host outputs (mc_archive_decode_block / read_region / decode_chunk).
+    Closed loop by default (latency = the call); with arrival times (ns), each
+    call starts at its arrival or when the previous one returns, and latency
+    runs from the arrival."""
     host = [np.empty(n, np.uint8) for n in (4096, 128 ** 3, 256 ** 3)]
     lat, nbytes = [], 0
     t_all = time.perf_counter()
@@ -345,6 +356,10 @@ def plain_per_call(a, tr, outs, device):
         k, lod = int(tr.kind[i]), int(tr.lod[i])
         z, y, x, dz, dy, dx = (int(v) for v in tr.req[i, :6])
         t1 = time.perf_counter()
+        if arrivals is not None:
+            t1 = t_all + float(arrivals[i]) / 1e9
+            while time.perf_counter() < t1:
+                pass
         if device:
             if k == 0:
                 a.read_regions_dev(lod, [(z * 16, y * 16, x * 16)], 16, 16, 16, outs[0].data_ptr())
@@ -366,6 +381,9 @@ def plain_per_call(a, tr, outs, device):
     secs = time.perf_counter() - t_all
     api = ("mc_b200_read_regions_dev / mc_b200_decode_chunks_dev (device outputs)" if device else
            "mc_archive_decode_block / read_region / decode_chunk (host outputs)")
+    if arrivals is not None:
+        api += f", open loop at {len(tr) / (float(arrivals[-1]) / 1e9):.0f} req/s offered"
+        secs = max(secs, float(arrivals[-1]) / 1e9)
     return _lat_summary(tr, lat, nbytes, secs, api)
 
 
