@@ -103,7 +103,9 @@ struct SrvBatch {
     uint64_t seq = 0;
     int cls = 0;                              // request class (stream) of the batch
     cudaEvent_t decoded = nullptr;            // recorded once the batch's misses are in the cache
-    std::vector<cudaEvent_t> waits;           // decode events of other-class batches it reads after
+    std::atomic<uint64_t> launched{0};        // seq of the last use whose launch has returned
+    // other-class batches (and their seq) whose decodes this batch reads after
+    std::vector<std::pair<SrvBatch *, uint64_t>> waits;
     struct mc_b200_server *srv = nullptr;
 };
 
@@ -328,8 +330,8 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
             // misses of this chunk still being decoded by a batch of the other class
             SrvBatch *db = c->dec_batch;
             if (db && db->busy && db->cls != cls && db->seq == c->dec_seq &&
-                std::find(B.waits.begin(), B.waits.end(), db->decoded) == B.waits.end())
-                B.waits.push_back(db->decoded);
+                std::find(B.waits.begin(), B.waits.end(), std::make_pair(db, db->seq)) == B.waits.end())
+                B.waits.emplace_back(db, db->seq);
             p.g.table = c->table;
             if (c->resolved == (uint32_t)kGrid3) continue;
             const ChunkIndex &ix = chunk_index(a->base, co);
@@ -433,10 +435,15 @@ void CUDART_CB on_done(void *p) {
 // host copies, completion callback.
 bool launch(mc_b200_server *S, SrvBatch &B, Lane &L) {
     cudaStream_t s = S->stream[B.cls];
-    // after the archive mirror's sync and the other class's decodes it reads
+    // after the archive mirror's sync and the other class's decodes it reads;
+    // the other class's worker may still be enqueueing such a batch: its
+    // decode event exists once that launch has returned, which takes
+    // microseconds, so wait for that first
     if (!cuda_ok(cudaStreamWaitEvent(s, S->mirror_ev[B.cls], 0), "stream wait")) return false;
-    for (cudaEvent_t e : B.waits)
-        if (!cuda_ok(cudaStreamWaitEvent(s, e, 0), "stream wait")) return false;
+    for (auto &w : B.waits) {
+        while (w.first->launched.load(std::memory_order_acquire) < w.second) std::this_thread::yield();
+        if (!cuda_ok(cudaStreamWaitEvent(s, w.first->decoded, 0), "stream wait")) return false;
+    }
     const size_t nu = B.upd.size();
     if (nu) {
         if (!B.h_upd.ensure(sizeof(uint2) * nu) || !B.d_upd.ensure(sizeof(uint2) * nu)) return false;
@@ -551,6 +558,7 @@ void worker_main(mc_b200_server *S, int c) {
         fb->gpu_done = false;
         lk.unlock();
         const bool ok = launch(S, *fb, *L);
+        fb->launched.store(fb->seq, std::memory_order_release);   // its decode event is recorded (or it failed)
         lk.lock();
         if (!ok) {
             cudaStreamSynchronize(S->stream[c]);
