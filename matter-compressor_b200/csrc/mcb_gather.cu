@@ -74,9 +74,27 @@ __global__ void __launch_bounds__(128) k_gather_boxes(const GatherItem *items, i
             const int z = z0 + r / ny, y = y0 + r % ny;
             uint8_t *row = dst + z * it.sz + y * it.sy;
             const uint8_t *srow = src ? src + (z - bz * 16) * 256 + (y - by * 16) * 16 - bx * 16 : nullptr;
-            if (full_x && ((uintptr_t)(row + x0) & 15) == 0) {
-                *reinterpret_cast<uint4 *>(row + x0) =
-                    srow ? *reinterpret_cast<const uint4 *>(srow + x0) : make_uint4(0, 0, 0, 0);
+            if (full_x) {
+                // a whole 16-byte block row: one aligned load from the cache slot
+                const uint4 v = srow ? *reinterpret_cast<const uint4 *>(srow + x0) : make_uint4(0, 0, 0, 0);
+                uint8_t *d = row + x0;
+                const uint32_t mis = (uint32_t)(uintptr_t)d & 15;
+                if (mis == 0) {
+                    *reinterpret_cast<uint4 *>(d) = v;
+                } else if ((mis & 3) == 0) {
+                    uint32_t *dw = reinterpret_cast<uint32_t *>(d);
+                    dw[0] = v.x; dw[1] = v.y; dw[2] = v.z; dw[3] = v.w;
+                } else {
+                    // destination off a 4-byte boundary by s: the head's 4 - s
+                    // bytes, three aligned words of shifted source bytes, the
+                    // tail's s bytes
+                    const uint32_t sft = mis & 3, w[4] = {v.x, v.y, v.z, v.w};
+                    for (uint32_t i = 0; i < 4 - sft; ++i) d[i] = (uint8_t)(w[0] >> (8 * i));
+                    uint32_t *dw = reinterpret_cast<uint32_t *>(d + 4 - sft);
+#pragma unroll
+                    for (int j = 1; j < 4; ++j) dw[j - 1] = __funnelshift_r(w[j - 1], w[j], 8 * (4 - sft));
+                    for (uint32_t i = 0; i < sft; ++i) d[16 - sft + i] = (uint8_t)(w[3] >> (8 * (4 - sft + i)));
+                }
             } else {
                 for (int x = x0; x <= x1; ++x) row[x] = srow ? srow[x] : 0;
             }
