@@ -32,7 +32,7 @@ def _stale(obj, deps):
 
 def build(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "matter_compressor_b200.h"))
     objs = []
     for src in SOURCES:

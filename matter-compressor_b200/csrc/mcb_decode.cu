@@ -28,6 +28,7 @@
 #include "mcb_devinfo.h"
 #include "mcb_format.h"
 #include "mcb_kernels.h"
+#include "mcb_rowstore.cuh"
 
 namespace mcb {
 
@@ -897,8 +898,8 @@ __device__ __forceinline__ void store_block(const DecItem &it, const uint8_t *st
         const int z = z0 + r / ny, y = y0 + r % ny;
         uint8_t *row = dst + z * it.sz + y * it.sy;
         const uint8_t *srow = stage + z * kStageZ + y * 16;
-        if (x0 == 0 && x1 == 15 && ((uintptr_t)row & 15) == 0) {
-            *reinterpret_cast<uint4 *>(row) = *reinterpret_cast<const uint4 *>(srow);
+        if (x0 == 0 && x1 == 15) {
+            store_row16(row, *reinterpret_cast<const uint4 *>(srow));
         } else {
             for (int x = x0; x <= x1; ++x) row[x] = srow[x];
         }

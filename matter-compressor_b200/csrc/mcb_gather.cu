@@ -6,13 +6,14 @@
 // coordinates, and the output address of chunk-local voxel (0,0,0). Every
 // resident chunk owns a table of 4096 cache-slot numbers in device memory;
 // kZeroSlot marks an absent (all-air) block. The gather flattens all items'
-// blocks into one index space; each warp copies one contiguous run of it.
+// blocks into one index space and copies one block per warp.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "mcb_devinfo.h"
 #include "mcb_format.h"
 #include "mcb_kernels.h"
+#include "mcb_rowstore.cuh"
 
 namespace mcb {
 
@@ -26,34 +27,16 @@ __global__ void __launch_bounds__(256) k_table_update(const uint2 *upd, int n, u
 __global__ void __launch_bounds__(128) k_gather_boxes(const GatherItem *items, int nitems, uint32_t nblocks,
                                                       const uint32_t *tables, const uint8_t *cache) {
     const int lane = threadIdx.x & 31;
-    // each warp copies one contiguous run of flattened blocks: x-adjacent
-    // blocks of an item follow each other, so the 16-byte row pieces of
-    // neighbouring blocks reach L2 close together and fill whole sectors, and
-    // the item holding a block is found by one search per warp, then by
-    // stepping forward
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const uint32_t per = (nblocks + nwarps - 1) / nwarps;
-    const uint32_t g0 = w * per, g1 = min(nblocks, g0 + per);
-    if (g0 >= g1) return;
-    int cur;
-    {   // the last item whose first <= g0
+    for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nblocks; g += nwarps) {
+        // the item holding flattened block g: the last one whose first <= g
         int lo = 0, hi = nitems - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].first <= g0) lo = mid;
+            if (items[mid].first <= g) lo = mid;
             else hi = mid - 1;
         }
-        cur = lo;
-    }
-    GatherItem it = items[cur];
-    uint32_t next_first = cur + 1 < nitems ? items[cur + 1].first : 0xFFFFFFFFu;
-    for (uint32_t g = g0; g < g1; ++g) {
-        while (g >= next_first) {
-            ++cur;
-            it = items[cur];
-            next_first = cur + 1 < nitems ? items[cur + 1].first : 0xFFFFFFFFu;
-        }
+        const GatherItem it = items[lo];
         const uint32_t local = g - it.first;
         const int bz0 = it.box_lo >> 8, by0 = (it.box_lo >> 4) & 15, bx0 = it.box_lo & 15;
         const int nby = ((it.box_hi >> 4) & 15) - by0 + 1, nbx = (it.box_hi & 15) - bx0 + 1;
@@ -74,27 +57,8 @@ __global__ void __launch_bounds__(128) k_gather_boxes(const GatherItem *items, i
             const int z = z0 + r / ny, y = y0 + r % ny;
             uint8_t *row = dst + z * it.sz + y * it.sy;
             const uint8_t *srow = src ? src + (z - bz * 16) * 256 + (y - by * 16) * 16 - bx * 16 : nullptr;
-            if (full_x) {
-                // a whole 16-byte block row: one aligned load from the cache slot
-                const uint4 v = srow ? *reinterpret_cast<const uint4 *>(srow + x0) : make_uint4(0, 0, 0, 0);
-                uint8_t *d = row + x0;
-                const uint32_t mis = (uint32_t)(uintptr_t)d & 15;
-                if (mis == 0) {
-                    *reinterpret_cast<uint4 *>(d) = v;
-                } else if ((mis & 3) == 0) {
-                    uint32_t *dw = reinterpret_cast<uint32_t *>(d);
-                    dw[0] = v.x; dw[1] = v.y; dw[2] = v.z; dw[3] = v.w;
-                } else {
-                    // destination off a 4-byte boundary by s: the head's 4 - s
-                    // bytes, three aligned words of shifted source bytes, the
-                    // tail's s bytes
-                    const uint32_t sft = mis & 3, w[4] = {v.x, v.y, v.z, v.w};
-                    for (uint32_t i = 0; i < 4 - sft; ++i) d[i] = (uint8_t)(w[0] >> (8 * i));
-                    uint32_t *dw = reinterpret_cast<uint32_t *>(d + 4 - sft);
-#pragma unroll
-                    for (int j = 1; j < 4; ++j) dw[j - 1] = __funnelshift_r(w[j - 1], w[j], 8 * (4 - sft));
-                    for (uint32_t i = 0; i < sft; ++i) d[16 - sft + i] = (uint8_t)(w[3] >> (8 * (4 - sft + i)));
-                }
+            if (full_x) {   // a whole 16-byte block row: one aligned load from the cache slot
+                store_row16(row + x0, srow ? *reinterpret_cast<const uint4 *>(srow + x0) : make_uint4(0, 0, 0, 0));
             } else {
                 for (int x = x0; x <= x1; ++x) row[x] = srow ? srow[x] : 0;
             }
@@ -115,11 +79,9 @@ cudaError_t launch_table_update(const uint2 *d_upd, int n, uint32_t *d_tables, c
 cudaError_t launch_gather_boxes(const GatherItem *d_items, int nitems, uint32_t nblocks, const uint32_t *d_tables,
                                 const uint8_t *d_cache, cudaStream_t s) {
     if (nitems <= 0 || nblocks == 0) return cudaSuccess;
-    // at least 8 blocks per warp where the batch allows; at most 8 CTAs per SM
-    uint32_t blocks = (nblocks + 31) / 32;
+    uint32_t blocks = (nblocks + 3) / 4;   // a block per warp, at most 8 CTAs per SM
     const uint32_t cap = (uint32_t)sm_count() * 8;
     if (blocks > cap) blocks = cap;
-    if (blocks == 0) blocks = 1;
     k_gather_boxes<<<blocks, 128, 0, s>>>(d_items, nitems, nblocks, d_tables, d_cache);
     return cudaGetLastError();
 }
