@@ -947,8 +947,9 @@ def run_b200(args, d):
     layout_ms = {}
     tuned = [plan_cfg[k] for k in ("entropy_warps_per_cta", "entropy_ctas_per_sm", "entropy_claim",
                                    "reconstruct_ctas_per_sm")]
+    solo = plan_cfg["entropy_solo_share"]
     for stages in plan.STAGES:
-        if plan.set_tuning(*tuned, stages) != 0:
+        if plan.set_tuning(*tuned, stages, solo) != 0:
             continue
         for k in range(2):
             plan.launch(s.cuda_stream)
@@ -962,7 +963,7 @@ def run_b200(args, d):
             torch.cuda.synchronize()
             tot += e0.elapsed_time(e1)
         layout_ms[stages] = round(tot / args.steps, 4)
-    plan.set_tuning(*tuned, plan_cfg["stages"])
+    plan.set_tuning(*tuned, plan_cfg["stages"], solo)
     plan.launch(s.cuda_stream)
     torch.cuda.synchronize()
 

@@ -205,11 +205,14 @@ int  mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]);
  * own batch (cached per quality and batch size): out[0] entropy warps per CTA
  * (2, 4, 8), out[1] entropy CTAs per SM, out[2] entropy queue claim run
  * (entries a lane takes per claim), out[3] reconstruction CTAs per SM,
- * out[4] the stage layout as in mc_b200_plan_config. */
-void mc_b200_plan_tuning(const mc_b200_plan *p, int out[5]);
+ * out[4] the stage layout as in mc_b200_plan_config, out[5] the single-thread
+ * share: the longest coded/out[5] blocks of a launch are entropy-decoded one
+ * per warp by one thread, at a few times a shared lane's speed per bin
+ * (0: none; at most half of the launch's warps). */
+void mc_b200_plan_tuning(const mc_b200_plan *p, int out[6]);
 /* Replace it (same layout; warps x CTAs per SM at most 25) and recapture the
  * plan. 0 on success, -1 on bad arguments or a CUDA error. */
-int  mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[5]);
+int  mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[6]);
 /* Fused layout only: how many times (each a sleep of at most 1 us) a CTA
  * polls a completion-list position that no block pair has filled yet before
  * it hands the position to the tail kernel and leaves (default 32768). Any

@@ -207,6 +207,10 @@ LaunchCfg autotune(DecodeBatch &B, float q, int nblocks, cudaStream_t s) {
     pick(8, [](LaunchCfg &c, int i) { c.ent_warps = ent_shape[i][0]; c.ent_ctas_per_sm = ent_shape[i][1]; }, 0);
     static const int ent_claim[] = {1, 2, 4};
     pick(3, [](LaunchCfg &c, int i) { c.ent_claim = ent_claim[i]; }, 0);
+    // the longest 1/64 .. 1/8 of the blocks on single-thread warps, none, or
+    // all of them (the single-thread kernel)
+    static const int ent_solo[] = {0, 64, 32, 16, 8, 1};
+    pick(6, [](LaunchCfg &c, int i) { c.ent_solo = ent_solo[i]; }, 0);
     static const int rec_opts[] = {3, 4, 5};
     pick(3, [](LaunchCfg &c, int i) { c.rec_ctas_per_sm = rec_opts[i]; }, 1);
     // the whole decode: separate kernels, the long blocks on a second
@@ -304,7 +308,7 @@ void mc_archive_decode_block(mc_archive *a, uint64_t co, int bz, int by, int bx,
     if (!L) { memset(dst, 0, kN3); return; }
     const int slot = qslot(sanitize_q(chunk_q(a, co)));
     uint8_t *dbase = slot < 0 ? nullptr : mirror_sync(a, *L);
-    if (!dbase || !L->out.ensure(kN3) || !L->h_stage.ensure(kN3)) { memset(dst, 0, kN3); return; }
+    if (!dbase) { memset(dst, 0, kN3); return; }
     const ChunkIndex &ix = chunk_index(a->base, co);
     const int bi = (bz * 16 + by) * 16 + bx;
     DecItem it;
@@ -313,19 +317,10 @@ void mc_archive_decode_block(mc_archive *a, uint64_t co, int bz, int by, int bx,
         it.src = dptr(dbase + ix.off[bi]);
         it.len = ix.len[bi];
     }
-    it.dst = dptr(L->out.p);
-    it.sz = 256;
-    it.sy = 16;
     it.qslot = (uint16_t)slot;
     it.clip_lo = kClipFullLo;
     it.clip_hi = kClipFullHi;
-    if (!decode_one(*L, it) ||
-        !cuda_ok(cudaMemcpyAsync(L->h_stage.p, L->out.p, kN3, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
-        !finish(*L, nullptr)) {
-        memset(dst, 0, kN3);
-        return;
-    }
-    memcpy(dst, L->h_stage.p, kN3);
+    if (!decode_one_host(*L, it, dst)) memset(dst, 0, kN3);
 }
 
 void mc_archive_decode_chunk(mc_archive *a, uint64_t co, mc_u8 *out, int nthreads) {
@@ -687,18 +682,19 @@ int mc_b200_plan_set_config(mc_b200_plan *p, const int cfg[3]) {
     return plan_capture(p) ? 0 : -1;
 }
 
-void mc_b200_plan_tuning(const mc_b200_plan *p, int out[5]) {
+void mc_b200_plan_tuning(const mc_b200_plan *p, int out[6]) {
     if (!out) return;
     out[0] = p ? p->cfg.ent_warps : 0;
     out[1] = p ? p->cfg.ent_ctas_per_sm : 0;
     out[2] = p ? p->cfg.ent_claim : 0;
     out[3] = p ? p->cfg.rec_ctas_per_sm : 0;
     out[4] = p ? (p->cfg.fused ? 2 : (int)p->cfg.split) : 0;
+    out[5] = p ? p->cfg.ent_solo : 0;
 }
 
-int mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[5]) {
+int mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[6]) {
     if (!p || !cfg || (cfg[0] != 2 && cfg[0] != 4 && cfg[0] != 8) || cfg[1] < 1 || cfg[0] * cfg[1] > 25 ||
-        cfg[2] < 1 || cfg[2] > 64 || cfg[3] < 1 || cfg[3] > 16 || cfg[4] < 0 || cfg[4] > 2) {
+        cfg[2] < 1 || cfg[2] > 64 || cfg[3] < 1 || cfg[3] > 16 || cfg[4] < 0 || cfg[4] > 2 || cfg[5] < 0) {
         set_error("plan_set_tuning: bad arguments");
         return -1;
     }
@@ -709,6 +705,7 @@ int mc_b200_plan_set_tuning(mc_b200_plan *p, const int cfg[5]) {
     c.rec_ctas_per_sm = cfg[3];
     c.split = cfg[4] == 1;
     c.fused = cfg[4] == 2;
+    c.ent_solo = cfg[5];
     if (c.fused && fused_grid(c) <= 0) {
         set_error("plan_set_tuning: the fused kernel cannot launch on this device");
         return -1;

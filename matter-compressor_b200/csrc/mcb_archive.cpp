@@ -461,7 +461,7 @@ void mc_dec_block(mc_codec_ctx *C, const mc_u8 *p, uint32_t plen, mc_u8 *dst) {
     if (!L || !C) { memset(dst, 0, kN3); return; }
     int slot = qslot(C->quality);
     if (slot < 0 || !cuda_ok(cudaEventSynchronize(L->done), "sync") || !L->src.ensure(plen + 64) ||
-        !L->out.ensure(kN3) || !L->h_stage.ensure(plen + kN3 + 64)) {
+        !L->h_stage.ensure(plen + 64)) {
         memset(dst, 0, kN3);
         return;
     }
@@ -469,21 +469,13 @@ void mc_dec_block(mc_codec_ctx *C, const mc_u8 *p, uint32_t plen, mc_u8 *dst) {
     if (plen) memcpy(hs, p, plen);
     DecItem it{};
     it.src = (uint64_t)(uintptr_t)L->src.p;
-    it.dst = (uint64_t)(uintptr_t)L->out.p;
-    it.sz = 256;
-    it.sy = 16;
     it.len = plen;
     it.qslot = (uint16_t)slot;
     it.clip_lo = kClipFullLo;
     it.clip_hi = kClipFullHi;
     if ((plen && !cuda_ok(cudaMemcpyAsync(L->src.p, hs, plen, cudaMemcpyHostToDevice, L->stream), "H2D")) ||
-        !decode_one(*L, it) ||
-        !cuda_ok(cudaMemcpyAsync(hs, L->out.p, kN3, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
-        !cuda_ok(cudaStreamSynchronize(L->stream), "sync")) {
+        !decode_one_host(*L, it, dst))
         memset(dst, 0, kN3);
-        return;
-    }
-    memcpy(dst, hs, kN3);
 }
 
 // ================================================================= archive

@@ -421,7 +421,7 @@ __device__ __forceinline__ void fast_step(LaneState &L, const EntParams &P, uint
     const bool bit = L.code >= r0;
     const uint32_t code = bit ? L.code - r0 : L.code;
     const uint32_t range = (bit & !is_byp) ? L.range - r0 : r0;
-    const uint32_t np0 = pc + (uint32_t)((int)((bit ? 15u : 4096u) - pc) >> 4);
+    const uint32_t np0 = (15u * pc + (bit ? 15u : 4096u)) >> 4;   // p - (p >> 4) or p + ((4096 - p) >> 4)
     ctx[cc * 32] = np0;   // bypass bins write the scratch slot
     // renormalisation, first byte (src/mc_codec.c:202); not between the bits
     // of a suffix
@@ -479,7 +479,8 @@ __device__ __forceinline__ int claim_next(Claim &c, const EntParams &P, int nlan
     return c.next++;
 }
 
-// Every lane of the warp decodes blocks until the queue is empty. Fast steps
+// Every lane of the warp decodes blocks until the queue is empty. Lane gtid
+// starts with entry gtid (none when gtid < 0), then claims from the counter. Fast steps
 // run while every lane is in a fast state or parked; when a lane reaches a
 // slow state the warp leaves the loop, that lane works its slow states off
 // (finishing its block and starting the next one), and the loop resumes.
@@ -493,7 +494,7 @@ __device__ __forceinline__ void run_lanes(LaneState &L, const EntParams &P, uint
     memset(&L, 0, sizeof L);
     park(L);
     L.st = S_DONE;
-    Claim c{gtid, gtid + 1};
+    Claim c = gtid >= 0 ? Claim{gtid, gtid + 1} : Claim{0, 0};   // gtid < 0: queue claims only
     for (;;) {
         // two steps per loop turn (the loop-carried lane state then needs
         // no register shuffling between the two), the check after each
@@ -520,6 +521,139 @@ __device__ __forceinline__ void run_lanes(LaneState &L, const EntParams &P, uint
     }
 }
 
+// The whole stream of one block on one thread, after lane_begin, written for
+// the latency of one thread alone on its warp (no other lane shares its
+// instructions). All contexts of the coefficient loop that the common bins
+// use are held in registers: the four significance contexts of the current
+// band (the one in use as a live probability, written back when the density
+// changes) and the twelve magnitude rungs. A run of insignificant positions
+// then costs per bin the range split, the compare, the probability update
+// and the loop's exit test; the flag that leaves the 16-position density
+// window, a renormalisation and the end of the band or the scan leave the
+// run. Band changes, renormalisation, Exp-Golomb tails and the corrections
+// take the shared step functions (position_event, renorm, eg_value,
+// put_entry, slow_work). Bands only advance, so a band's register contexts
+// are never written back to shared memory, and the magnitude rungs are used
+// by nothing else.
+__device__ __forceinline__ uint32_t pick4(uint32_t c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3) {
+    return c == 0 ? a0 : (c == 1 ? a1 : (c == 2 ? a2 : a3));
+}
+// p + ((4096 - p) >> 4) and p - (p >> 4) (src/mc_codec.c:198-204) as one
+// multiply-add and a shift: equal for every p in 0..4096
+__device__ __forceinline__ uint32_t prob_after0(uint32_t p) { return (15u * p + 4096u) >> 4; }
+__device__ __forceinline__ uint32_t prob_after1(uint32_t p) { return (15u * p + 15u) >> 4; }
+// One magnitude rung on a register context; after a 1 the range is
+// renormalised here, after the closing 0 by the caller.
+__device__ __forceinline__ bool rung(LaneState &L, uint32_t &g) {
+    const uint32_t r = (L.range >> 12) * g;
+    if (L.code < r) {
+        L.range = r;
+        g = prob_after0(g);
+        return false;
+    }
+    L.code -= r;
+    L.range -= r;
+    g = prob_after1(g);
+    if (L.range < (1u << 24)) renorm(L);
+    return true;
+}
+
+__device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, uint32_t *ctx,
+                                             const uint16_t *s_bend) {
+    uint32_t sigb = L.sigb;
+    uint32_t s0 = ctx[(sigb + 0) * 32], s1 = ctx[(sigb + 1) * 32];
+    uint32_t s2 = ctx[(sigb + 2) * 32], s3 = ctx[(sigb + 3) * 32];
+    uint32_t g0 = ctx[(kCtxMag + 0) * 32], g1 = ctx[(kCtxMag + 1) * 32], g2 = ctx[(kCtxMag + 2) * 32];
+    uint32_t g3 = ctx[(kCtxMag + 3) * 32], g4 = ctx[(kCtxMag + 4) * 32], g5 = ctx[(kCtxMag + 5) * 32];
+    uint32_t g6 = ctx[(kCtxMag + 6) * 32], g7 = ctx[(kCtxMag + 7) * 32], g8 = ctx[(kCtxMag + 8) * 32];
+    uint32_t g9 = ctx[(kCtxMag + 9) * 32], g10 = ctx[(kCtxMag + 10) * 32], g11 = ctx[(kCtxMag + 11) * 32];
+    uint32_t h = L.hist & 0xFFFFu;   // the last 16 significance flags, newest in bit 0
+    uint32_t cnt = __popc(h);
+    // a position event; the band's contexts come into registers when it changes
+    auto event = [&]() {
+        L.hist = h;
+        position_event(L, ctx, s_bend);
+        if (L.sigb != sigb) {
+            sigb = L.sigb;
+            s0 = ctx[(sigb + 0) * 32]; s1 = ctx[(sigb + 1) * 32];
+            s2 = ctx[(sigb + 2) * 32]; s3 = ctx[(sigb + 3) * 32];
+        }
+        h = L.hist & 0xFFFFu;
+        cnt = __popc(h);
+    };
+    while (L.st <= F_MAG) {   // lane_begin leaves F_SIG, F_MAG or a slow state
+        if (L.st == F_SIG) {   // L.p < L.stop
+            const uint32_t c = min(cnt, 3u);
+            uint32_t pc = pick4(c, s0, s1, s2, s3);
+            uint32_t code = L.code, range = L.range, p = L.p;
+            const uint32_t stop = L.stop;
+            // a run of bins with one exit test each: every bin updates the
+            // state the same way, by selects on its value; the run ends on a
+            // significant bin, a renormalisation, the end of the band or scan,
+            // or a flag leaving the density window
+            bool sig;
+            for (;;) {
+                const uint32_t r0 = (range >> 12) * pc;
+                sig = code >= r0;
+                code = sig ? code - r0 : code;
+                range = sig ? range - r0 : r0;
+                pc = (15u * pc + (sig ? 15u : 4096u)) >> 4;
+                h = (h << 1) | (sig ? 1u : 0u);
+                p += sig ? 0u : 1u;
+                if (sig | (range < (1u << 24)) | (p >= stop) | (h > 0xFFFFu)) break;
+            }
+            s0 = c == 0 ? pc : s0; s1 = c == 1 ? pc : s1;
+            s2 = c == 2 ? pc : s2; s3 = c == 3 ? pc : s3;
+            L.code = code;
+            L.range = range;
+            L.p = p;
+            cnt = cnt + (sig ? 1u : 0u) - (h >> 16);   // the flag that entered, the one that left
+            h &= 0xFFFFu;
+            if (L.range < (1u << 24)) renorm(L);
+            if (sig) L.st = F_MAG;
+            else if (L.p >= L.stop) event();
+            continue;
+        }
+        // F_MAG: the unary magnitude (src/mc_codec.c:268-275), then the sign
+        // and the coefficient's entry
+        uint32_t m;
+        const uint32_t r = (L.range >> 12) * g0;   // rung 0, by selects
+        const bool b0 = L.code >= r;
+        L.code = b0 ? L.code - r : L.code;
+        L.range = b0 ? L.range - r : r;
+        g0 = (15u * g0 + (b0 ? 15u : 4096u)) >> 4;
+        if (L.range < (1u << 24)) renorm(L);
+        if (!b0) m = 1;
+        else if (!rung(L, g1)) m = 2;
+        else if (!rung(L, g2)) m = 3;
+        else if (!rung(L, g3)) m = 4;
+        else if (!rung(L, g4)) m = 5;
+        else if (!rung(L, g5)) m = 6;
+        else if (!rung(L, g6)) m = 7;
+        else if (!rung(L, g7)) m = 8;
+        else if (!rung(L, g8)) m = 9;
+        else if (!rung(L, g9)) m = 10;
+        else if (!rung(L, g10)) m = 11;
+        else if (!rung(L, g11)) m = 12;
+        else m = 0;
+        if (m == 0) {   // the twelfth rung set: 12 + an Exp-Golomb value
+            m = 12u + eg_value(L);
+            if (L.bad) { L.st = S_DONE; break; }   // prefix cap (corrupt stream)
+        } else if (L.range < (1u << 24)) {
+            renorm(L);
+        }
+        L.range >>= 1;   // the sign, a bypass bin (src/mc_codec.c:205)
+        const bool neg = L.code >= L.range;
+        if (neg) L.code -= L.range;
+        if (L.range < (1u << 24)) renorm(L);
+        if (!put_entry(L, P, L.p | ((neg ? 0u - m : m) << 16))) break;   // pool exhausted: S_DONE
+        ++L.p;
+        L.st = F_SIG;
+        if (L.p >= L.stop) event();
+    }
+    while (L.st != S_DONE) slow_work(L, P, ctx, s_bend);
+}
+
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
     // s_bend[b]: first scan position past band b; then the lanes' contexts,
@@ -535,10 +669,58 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *ctx = s_ent + 8 + warp * kCtxSlots * 32 + lane;
     LaneState L;
-    run_lanes(L, P, ctx, s_bend, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, [](int) {});
+    // warps 0..nsolo-1 of the grid: order entry `warp` on the warp's first
+    // thread alone, then the queue
+    const int gwarp = blockIdx.x * WARPS + warp;
+    if (gwarp < P.nsolo) {
+        if (lane == 0) {
+            memset(&L, 0, sizeof L);
+            lane_begin(L, P, ctx, s_bend, (int)P.order[gwarp]);
+            solo_entropy(L, P, ctx, s_bend);
+            lane_finish(L, P);
+        }
+        __syncwarp();
+    }
+    EntParams F = P;   // the rest of the order, one lane per block
+    F.order = P.order ? P.order + P.nsolo : nullptr;
+    F.ncoded = P.ncoded - P.nsolo;
+    const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 32 * P.nsolo;
+    run_lanes(L, F, ctx, s_bend, gtid, (int)(gridDim.x * blockDim.x) - 32 * P.nsolo, [](int) {});
 }
 // dynamic shared memory of k_entropy<W>
 constexpr size_t entropy_smem(int warps) { return 32 + sizeof(uint32_t) * kCtxSlots * 32 * (size_t)warps; }
+
+// The entropy stage with every block on a single thread: each warp's first
+// thread decodes blocks of the order one after another (entry `warp` first,
+// then claims from the counter), the other 31 threads leave at once. A block
+// then costs a few times fewer cycles per bin than as a lane of k_entropy, at
+// several times the issue slots per bin, which pays where a batch is too
+// small to fill the machine and its longest blocks set the stage's time. The
+// threads' contexts share one 32-column region of shared memory (column =
+// warp index), conflict-free like k_entropy's. Two CTAs of 16 warps per SM
+// fit the register file at 64 registers a thread.
+constexpr int kSoloWarps = 16;
+__global__ void __launch_bounds__(kSoloWarps * 32, 2) k_entropy_solo(EntParams P) {
+    __shared__ uint32_t s_ctx[kCtxSlots * 32];
+    __shared__ uint16_t s_bend[9];
+    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
+        const uint32_t b = P.scan[i] >> 12;
+        if ((P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
+    }
+    if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
+    __syncthreads();
+    if (threadIdx.x & 31) return;
+    const int warp = threadIdx.x >> 5;
+    uint32_t *ctx = s_ctx + warp;
+    const int nwarps = gridDim.x * kSoloWarps;
+    for (int j = blockIdx.x * kSoloWarps + warp; j < P.ncoded; j = nwarps + (int)atomicAdd(P.counter, 1u)) {
+        LaneState L;
+        memset(&L, 0, sizeof L);
+        lane_begin(L, P, ctx, s_bend, P.order ? (int)P.order[j] : j);
+        solo_entropy(L, P, ctx, s_bend);
+        lane_finish(L, P);
+    }
+}
 
 // ---------------------------------------------------------------- stage 2
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -1135,17 +1317,6 @@ __global__ void __launch_bounds__(128) k_fused_tail(FusedParams F) {
 // warp step avoids by fetching both candidate contexts ahead, without
 // branches.
 
-// The whole stream of one block on one lane: fast steps, and the slow
-// states in between, until the block is done.
-__device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, uint32_t *ctx,
-                                             const uint16_t *s_bend) {
-    for (;;) {
-        while (L.st <= F_BYP) fast_step(L, P, ctx, s_bend);
-        if (L.st == S_DONE) return;
-        slow_work(L, P, ctx, s_bend);
-    }
-}
-
 static_assert(sizeof(DecItem) % 16 == 0, "SoloScratch::hdr must sit on a 16-byte boundary");
 
 __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, const QTab *qtab,
@@ -1235,17 +1406,29 @@ static cudaError_t launch_entropy_w(const EntParams &p, int ctas_per_sm, cudaStr
         return e == cudaSuccess ? 1 : -(int)e;
     });
     if (a < 0) return (cudaError_t)(-a);
-    int blocks = (p.ncoded + W * 32 - 1) / (W * 32);
+    // one warp per solo block, one lane per other block
+    EntParams q = p;
+    if (!q.order || q.nsolo < 0) q.nsolo = 0;
+    if (q.nsolo > q.ncoded) q.nsolo = q.ncoded;
+    int blocks = (q.nsolo + (q.ncoded - q.nsolo + 31) / 32 + W - 1) / W;
     const int cap = num_sms() * ctas_per_sm;
     if (blocks > cap) blocks = cap;
-    k_entropy<W><<<blocks, W * 32, entropy_smem(W), s>>>(p);
+    if (q.nsolo > blocks * W / 2) q.nsolo = blocks * W / 2;   // at most half of the warps
+    k_entropy<W><<<blocks, W * 32, entropy_smem(W), s>>>(q);
     return cudaGetLastError();
 }
 
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s) {
     if (p.ncoded <= 0) return cudaSuccess;
+    if (cfg.ent_solo == 1) {   // every block on a single thread
+        int blocks = (p.ncoded + kSoloWarps - 1) / kSoloWarps;
+        if (blocks > 2 * num_sms()) blocks = 2 * num_sms();
+        k_entropy_solo<<<blocks, kSoloWarps * 32, 0, s>>>(p);
+        return cudaGetLastError();
+    }
     EntParams q = p;
     q.claim = cfg.ent_claim > 0 ? cfg.ent_claim : 1;
+    q.nsolo = cfg.ent_solo > 0 ? p.ncoded / cfg.ent_solo : 0;
     const int per_sm = cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5;
     switch (cfg.ent_warps) {
     case 2: return launch_entropy_w<2>(q, per_sm, s);

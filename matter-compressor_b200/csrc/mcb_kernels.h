@@ -13,6 +13,9 @@ struct LaunchCfg {
     int ent_claim = 1;         // entropy stage: queue entries a lane claims at a time (1, 2 or 4)
     int ent_ctas_per_sm = 5;   // entropy stage: CTAs per SM (8.8 KB of contexts per warp)
     int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
+    int ent_solo = 0;          // entropy stage: the longest ncoded / ent_solo blocks are decoded one per
+                               // warp by a single thread (0: none; see EntParams::nsolo); 1: every
+                               // block, by the single-thread kernel k_entropy_solo
     bool split = false;        // long blocks on a second stream (batches large enough to split)
     bool fused = false;        // both stages in one persistent kernel (k_decode_fused)
     int fused_ctas_per_sm = 4;
@@ -38,6 +41,13 @@ struct EntParams {
     uint32_t *status;          // [0]: blocks whose stream was cut short, [1]: pool entries used
     uint32_t *counter;         // work counter of this launch, zero at launch
     int claim;                 // queue entries claimed per counter increment (>= 1)
+    // k_entropy: the first nsolo entries of the order (the longest payloads)
+    // are decoded one per warp by the warp's first thread alone, which gives a
+    // block's serial chain a few times the speed of a lane sharing its warp's
+    // instructions with 31 others; warps 0..nsolo-1 of the grid do this
+    // first, then join the other warps on the rest of the order. Needs an
+    // order and at most half of the launch's warps (launch_entropy clamps it).
+    int nsolo = 0;
 };
 
 struct RecParams {

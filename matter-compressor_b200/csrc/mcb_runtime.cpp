@@ -404,6 +404,30 @@ bool decode_one(Lane &L, const DecItem &it) {
            cuda_ok(cudaEventRecord(L.done, L.stream), "event record");
 }
 
+bool decode_one_host(Lane &L, DecItem it, uint8_t *dst) {
+    if (!L.h_one.ensure(kN3)) return false;
+    // pinned memory is mapped into the device's address space (unified
+    // addressing); the kernel's row stores cross the bus as posted writes
+    // when the device cannot address it, the block goes to device memory and
+    // comes back by one copy
+    void *d = nullptr;
+    const bool mapped = cudaHostGetDevicePointer(&d, L.h_one.p, 0) == cudaSuccess;
+    if (!mapped) {
+        cudaGetLastError();
+        if (!L.out.ensure(kN3)) return false;
+        d = L.out.p;
+    }
+    it.dst = (uint64_t)(uintptr_t)d;
+    it.sz = 256;
+    it.sy = 16;
+    if (!decode_one(L, it) ||
+        (!mapped && !cuda_ok(cudaMemcpyAsync(L.h_one.p, L.out.p, kN3, cudaMemcpyDeviceToHost, L.stream), "D2H")) ||
+        !cuda_ok(cudaStreamSynchronize(L.stream), "sync"))
+        return false;
+    memcpy(dst, L.h_one.p, kN3);
+    return true;
+}
+
 uint32_t lane_bad_blocks(Lane &L) {
     uint32_t v = 0;
     if (L.batch.status.p) cudaMemcpy(&v, L.batch.status.p, 4, cudaMemcpyDeviceToHost);

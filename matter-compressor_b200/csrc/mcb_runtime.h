@@ -109,6 +109,7 @@ struct Lane {
     DevBuf smp_grid, smp_cand, smp_acc;         // box sampling: block-fraction grid, candidates, accept flags
     DevBuf solo;                                // single-block decode scratch (SoloScratch)
     HostBuf h_items, h_base, h_stage, h_misc;
+    HostBuf h_one;                              // single-block output, written by the kernel over the bus
     LaunchCfg cfg;
     BlobSlot pipe[kBlobSlots];
     ~Lane();
@@ -134,6 +135,11 @@ bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s = nullptr
 // batch layout, no copies): the output lands at it.dst; the lane's status
 // word reports whether its stream was cut short.
 bool decode_one(Lane &L, const DecItem &it);
+// decode_one into host memory, synchronously: the kernel stores the 16^3
+// voxels straight into the lane's pinned, device-mapped output buffer (no
+// device-to-host copy is enqueued), then they are copied to dst. it.dst,
+// it.sz and it.sy are set here.
+bool decode_one_host(Lane &L, DecItem it, uint8_t *dst);
 
 // Encodes chunks of 256^3 voxels resident on the device (chunk c at
 // d_vox[c]) into assembled blobs. Synchronises; on return blob_len[c]

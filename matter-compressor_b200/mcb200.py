@@ -426,14 +426,16 @@ class Plan:
 
     def tuning(self):
         """The autotuner's full choice (mc_b200_plan_tuning)."""
-        out = np.zeros(5, np.int32)
+        out = np.zeros(6, np.int32)
         self.lib.L.mc_b200_plan_tuning(self.p, _ptr(out))
         return {"entropy_warps_per_cta": int(out[0]), "entropy_ctas_per_sm": int(out[1]),
                 "entropy_claim": int(out[2]), "reconstruct_ctas_per_sm": int(out[3]),
-                "stages": self.STAGES[int(out[4])]}
+                "stages": self.STAGES[int(out[4])], "entropy_solo_share": int(out[5])}
 
-    def set_tuning(self, warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, stages):
-        cfg = np.array([warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, self.STAGES.index(stages)], np.int32)
+    def set_tuning(self, warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, stages, solo_share=0):
+        """solo_share: the longest coded/solo_share blocks decoded one per warp by one thread (0: none)."""
+        cfg = np.array([warps, ctas_per_sm, claim, reconstruct_ctas_per_sm, self.STAGES.index(stages), solo_share],
+                       np.int32)
         rc = self.lib.L.mc_b200_plan_set_tuning(self.p, _ptr(cfg))
         self.lib.check()
         return rc

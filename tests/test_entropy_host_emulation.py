@@ -114,10 +114,10 @@ def _cut(src, start, end):
 
 def _host_source():
     src = open(os.path.join(CSRC, "mcb_decode.cu")).read()
-    stage1 = _cut(src, "// ---------------------------------------------------------------- stage 1",
-                  "template <int WARPS>\n__global__")
-    solo = _cut(src, "// The whole stream of one block on one lane", "static_assert(sizeof(DecItem)")
-    body = stage1 + solo
+    # stage 1 up to k_entropy: the lane step functions, run_lanes and the
+    # single-thread loop solo_entropy
+    body = _cut(src, "// ---------------------------------------------------------------- stage 1",
+                "template <int WARPS>\n__global__")
     for dev, host in (("__device__ __forceinline__", "static inline"), ("__ldg(", "LDG("),
                       ("atomicAdd(", "ATOMIC_ADD("), ("__byte_perm(", "BYTE_PERM("),
                       ("__popc(", "__builtin_popcount("), ("__any_sync(", "ANY_SYNC("),

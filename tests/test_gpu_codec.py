@@ -281,8 +281,9 @@ def test_fused_layout_gives_up_waiting(gpu, oracle, tmp_path):
 
 def test_plan_entropy_shapes(gpu, oracle, tmp_path):
     """Every entropy launch shape the autotuner may pick -- 2, 4 or 8 warps per
-    CTA, several CTAs per SM, queue claims of 1, 2 or 4 entries -- gives the
-    oracle's voxels, at three qualities in one batch."""
+    CTA, several CTAs per SM, queue claims of 1, 2 or 4 entries, the longest
+    blocks on single-thread warps or not -- gives the oracle's voxels, at three
+    qualities in one batch."""
     import torch
     import volumes
     with gpu.open(str(tmp_path / "e.mca"), 768, 256, 256, 6.0) as a:
@@ -297,13 +298,18 @@ def test_plan_entropy_shapes(gpu, oracle, tmp_path):
         try:
             t = plan.tuning()
             assert t["entropy_warps_per_cta"] in (2, 4, 8) and t["entropy_claim"] in (1, 2, 4)
-            for warps, ctas, claim in ((2, 12, 1), (4, 5, 2), (8, 3, 4), (4, 1, 1), (2, 3, 64)):
-                assert plan.set_tuning(warps, ctas, claim, 4, "sequential") == 0
+            # solo share: 1/16 of the blocks on single-thread warps; 2 asks for
+            # more than half of the warps and is clamped to that; 1 is the
+            # single-thread kernel
+            for warps, ctas, claim, solo in ((2, 12, 1, 0), (4, 5, 2, 16), (8, 3, 4, 0), (4, 1, 1, 2),
+                                             (2, 3, 64, 1), (4, 5, 1, 64)):
+                assert plan.set_tuning(warps, ctas, claim, 4, "sequential", solo) == 0
                 assert plan.tuning()["entropy_warps_per_cta"] == warps
+                assert plan.tuning()["entropy_solo_share"] == solo
                 d_out.fill_(0xEE)
                 plan.launch()
                 torch.cuda.synchronize()
-                assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim)
+                assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim, solo)
             with pytest.raises(RuntimeError, match="bad arguments"):   # 3 warps per CTA: refused
                 plan.set_tuning(3, 4, 1, 4, "sequential")
         finally:
