@@ -33,6 +33,9 @@
 namespace mcb {
 
 __constant__ float c_cos[16][16];
+// c_bend[b]: the first scan position past band b (b < 7), then kN3 and a
+// sentinel; kernels copy it into shared memory at start
+__constant__ uint16_t c_bend[9];
 
 // ---------------------------------------------------------------- stage 1
 // Lane states. The three fast states cover every bin of the coefficient loop
@@ -528,13 +531,15 @@ __device__ __forceinline__ void run_lanes(LaneState &L, const EntParams &P, uint
 // band (the one in use as a live probability, written back when the density
 // changes) and the twelve magnitude rungs. A run of insignificant positions
 // then costs per bin the range split, the compare, the probability update
-// and the loop's exit test; the flag that leaves the 16-position density
-// window, a renormalisation and the end of the band or the scan leave the
-// run. Band changes, renormalisation, Exp-Golomb tails and the corrections
-// take the shared step functions (position_event, renorm, eg_value,
-// put_entry, slow_work). Bands only advance, so a band's register contexts
-// are never written back to shared memory, and the magnitude rungs are used
-// by nothing else.
+// and one test for the rare events (a renormalisation, the flag that leaves
+// the 16-position density window, the end of the band or the scan). A
+// significant bin decodes its coefficient (magnitude, sign, entry) in place
+// and the run goes on; the common steps of a coefficient use selects rather
+// than branches, whose divergence bookkeeping costs more than their work.
+// Band changes, Exp-Golomb tails and the corrections take the shared step
+// functions (position_event, renorm, eg_value, put_entry, slow_work). Bands
+// only advance, so a band's register contexts are never written back to
+// shared memory, and the magnitude rungs are used by nothing else.
 __device__ __forceinline__ uint32_t pick4(uint32_t c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3) {
     return c == 0 ? a0 : (c == 1 ? a1 : (c == 2 ? a2 : a3));
 }
@@ -556,6 +561,19 @@ __device__ __forceinline__ bool rung(LaneState &L, uint32_t &g) {
     g = prob_after1(g);
     if (L.range < (1u << 24)) renorm(L);
     return true;
+}
+
+// Renormalisation with the common case (one byte, the window not emptied)
+// by selects; a second byte or a window refill takes the loop.
+__device__ __forceinline__ void renorm_sel(LaneState &L) {
+    const bool need = L.range < (1u << 24);
+    L.code = need ? __byte_perm(L.code, L.w, L.sel) : L.code;
+    L.range = need ? L.range << 8 : L.range;
+    L.sel += need ? 1u : 0u;
+    if ((L.sel == kSel0 + 4) | (L.range < (1u << 24))) {
+        if (L.sel == kSel0 + 4) refill(L);
+        renorm(L);
+    }
 }
 
 __device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, uint32_t *ctx,
@@ -581,75 +599,102 @@ __device__ __forceinline__ void solo_entropy(LaneState &L, const EntParams &P, u
         h = L.hist & 0xFFFFu;
         cnt = __popc(h);
     };
-    while (L.st <= F_MAG) {   // lane_begin leaves F_SIG, F_MAG or a slow state
-        if (L.st == F_SIG) {   // L.p < L.stop
-            const uint32_t c = min(cnt, 3u);
-            uint32_t pc = pick4(c, s0, s1, s2, s3);
-            uint32_t code = L.code, range = L.range, p = L.p;
-            const uint32_t stop = L.stop;
-            // a run of bins with one exit test each: every bin updates the
-            // state the same way, by selects on its value; the run ends on a
-            // significant bin, a renormalisation, the end of the band or scan,
-            // or a flag leaving the density window
-            bool sig;
-            for (;;) {
-                const uint32_t r0 = (range >> 12) * pc;
-                sig = code >= r0;
-                code = sig ? code - r0 : code;
-                range = sig ? range - r0 : r0;
-                pc = (15u * pc + (sig ? 15u : 4096u)) >> 4;
-                h = (h << 1) | (sig ? 1u : 0u);
-                p += sig ? 0u : 1u;
-                if (sig | (range < (1u << 24)) | (p >= stop) | (h > 0xFFFFu)) break;
-            }
-            s0 = c == 0 ? pc : s0; s1 = c == 1 ? pc : s1;
-            s2 = c == 2 ? pc : s2; s3 = c == 3 ? pc : s3;
-            L.code = code;
-            L.range = range;
-            L.p = p;
-            cnt = cnt + (sig ? 1u : 0u) - (h >> 16);   // the flag that entered, the one that left
-            h &= 0xFFFFu;
-            if (L.range < (1u << 24)) renorm(L);
-            if (sig) L.st = F_MAG;
-            else if (L.p >= L.stop) event();
-            continue;
-        }
-        // F_MAG: the unary magnitude (src/mc_codec.c:268-275), then the sign
-        // and the coefficient's entry
+    // the coefficient at L.p, known significant: the unary magnitude
+    // (src/mc_codec.c:268-275), the sign, the entry, the next position;
+    // false when the block ends (an Exp-Golomb prefix at the cap or the
+    // overflow pool exhausted: corrupt streams only)
+    auto coef = [&]() -> bool {
         uint32_t m;
         const uint32_t r = (L.range >> 12) * g0;   // rung 0, by selects
         const bool b0 = L.code >= r;
         L.code = b0 ? L.code - r : L.code;
         L.range = b0 ? L.range - r : r;
         g0 = (15u * g0 + (b0 ? 15u : 4096u)) >> 4;
-        if (L.range < (1u << 24)) renorm(L);
-        if (!b0) m = 1;
-        else if (!rung(L, g1)) m = 2;
-        else if (!rung(L, g2)) m = 3;
-        else if (!rung(L, g3)) m = 4;
-        else if (!rung(L, g4)) m = 5;
-        else if (!rung(L, g5)) m = 6;
-        else if (!rung(L, g6)) m = 7;
-        else if (!rung(L, g7)) m = 8;
-        else if (!rung(L, g8)) m = 9;
-        else if (!rung(L, g9)) m = 10;
-        else if (!rung(L, g10)) m = 11;
-        else if (!rung(L, g11)) m = 12;
-        else m = 0;
-        if (m == 0) {   // the twelfth rung set: 12 + an Exp-Golomb value
-            m = 12u + eg_value(L);
-            if (L.bad) { L.st = S_DONE; break; }   // prefix cap (corrupt stream)
-        } else if (L.range < (1u << 24)) {
+        renorm_sel(L);
+        if (!b0) {
+            m = 1;
+        } else {
+            if (!rung(L, g1)) m = 2;
+            else if (!rung(L, g2)) m = 3;
+            else if (!rung(L, g3)) m = 4;
+            else if (!rung(L, g4)) m = 5;
+            else if (!rung(L, g5)) m = 6;
+            else if (!rung(L, g6)) m = 7;
+            else if (!rung(L, g7)) m = 8;
+            else if (!rung(L, g8)) m = 9;
+            else if (!rung(L, g9)) m = 10;
+            else if (!rung(L, g10)) m = 11;
+            else if (!rung(L, g11)) m = 12;
+            else m = 0;
+            if (m == 0) {   // the twelfth rung set: 12 + an Exp-Golomb value
+                m = 12u + eg_value(L);
+                if (L.bad) { L.st = S_DONE; return false; }   // prefix cap
+            }
             renorm(L);
         }
         L.range >>= 1;   // the sign, a bypass bin (src/mc_codec.c:205)
         const bool neg = L.code >= L.range;
-        if (neg) L.code -= L.range;
-        if (L.range < (1u << 24)) renorm(L);
-        if (!put_entry(L, P, L.p | ((neg ? 0u - m : m) << 16))) break;   // pool exhausted: S_DONE
+        L.code = neg ? L.code - L.range : L.code;
+        renorm_sel(L);
+        const uint32_t v = L.p | ((neg ? 0u - m : m) << 16);
+        if (L.nent < L.cap) {
+            L.ent[L.nent++] = v;
+        } else if (!put_entry(L, P, v)) {
+            return false;   // S_DONE
+        }
         ++L.p;
         L.st = F_SIG;
         if (L.p >= L.stop) event();
+        return true;
+    };
+    for (;;) {
+        if (L.st == F_MAG) {   // the implicit last position (lane_begin or an event)
+            if (!coef()) break;
+            continue;
+        }
+        if (L.st != F_SIG) break;
+        // a run of significance bins at L.p < L.stop, the context in use as
+        // the live probability pc
+        uint32_t c = min(cnt, 3u);
+        uint32_t pc = pick4(c, s0, s1, s2, s3);
+        for (;;) {
+            const uint32_t r0 = (L.range >> 12) * pc;
+            if (L.code >= r0) {   // significant
+                L.code -= r0;
+                L.range -= r0;
+                pc = prob_after1(pc);
+                s0 = c == 0 ? pc : s0; s1 = c == 1 ? pc : s1;
+                s2 = c == 2 ? pc : s2; s3 = c == 3 ? pc : s3;
+                h = (h << 1) | 1u;
+                cnt += 1u - (h >> 16);   // the flag that entered, the one that left
+                h &= 0xFFFFu;
+                renorm_sel(L);
+                if (!coef()) break;
+                if (L.st != F_SIG) break;
+                c = min(cnt, 3u);
+                pc = pick4(c, s0, s1, s2, s3);
+                continue;
+            }
+            L.range = r0;
+            pc = prob_after0(pc);
+            h <<= 1;
+            ++L.p;
+            if ((L.range < (1u << 24)) | (L.p >= L.stop) | (h > 0xFFFFu)) {
+                if (L.range < (1u << 24)) renorm(L);
+                if ((L.p >= L.stop) | (h > 0xFFFFu)) {
+                    s0 = c == 0 ? pc : s0; s1 = c == 1 ? pc : s1;
+                    s2 = c == 2 ? pc : s2; s3 = c == 3 ? pc : s3;
+                    cnt -= h >> 16;   // the flag that left the window
+                    h &= 0xFFFFu;
+                    if (L.p >= L.stop) {
+                        event();
+                        if (L.st != F_SIG) break;
+                    }
+                    c = min(cnt, 3u);
+                    pc = pick4(c, s0, s1, s2, s3);
+                }
+            }
+        }
     }
     while (L.st != S_DONE) slow_work(L, P, ctx, s_bend);
 }
@@ -660,11 +705,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_entropy(EntParams P) {
     // context j of lane l of warp w at word (w * kCtxSlots + j) * 32 + l
     extern __shared__ uint32_t s_ent[];
     uint16_t *s_bend = reinterpret_cast<uint16_t *>(s_ent);
-    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
-        const uint32_t b = P.scan[i] >> 12;
-        if ((P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
-    }
-    if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
+    if (threadIdx.x < 9) s_bend[threadIdx.x] = c_bend[threadIdx.x];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *ctx = s_ent + 8 + warp * kCtxSlots * 32 + lane;
@@ -703,11 +744,7 @@ constexpr int kSoloWarps = 16;
 __global__ void __launch_bounds__(kSoloWarps * 32, 2) k_entropy_solo(EntParams P) {
     __shared__ uint32_t s_ctx[kCtxSlots * 32];
     __shared__ uint16_t s_bend[9];
-    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
-        const uint32_t b = P.scan[i] >> 12;
-        if ((P.scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
-    }
-    if (threadIdx.x == 0) { s_bend[7] = kN3; s_bend[8] = 0xFFFF; }
+    if (threadIdx.x < 9) s_bend[threadIdx.x] = c_bend[threadIdx.x];
     __syncthreads();
     if (threadIdx.x & 31) return;
     const int warp = threadIdx.x >> 5;
@@ -1228,15 +1265,11 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
     const int nlanes = gridDim.x * blockDim.x;
     // absent blocks are ready at once
     for (int q = P.ncoded + gtid; q < P.n; q += nlanes) pair_ready(F, (int)P.order[q]);
-    for (int i = threadIdx.x + 1; i < kN3; i += blockDim.x) {
-        const uint32_t b = P.scan[i] >> 12;
-        if ((P.scan[i - 1] >> 12) != b) S.u.e.bend[b - 1] = (uint16_t)i;
-    }
+    if (threadIdx.x < 9) S.u.e.bend[threadIdx.x] = c_bend[threadIdx.x];
     for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         S.W[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
     }
-    if (threadIdx.x == 0) { S.u.e.bend[7] = kN3; S.u.e.bend[8] = 0xFFFF; }
     __syncthreads();
 
     // ---- entropy: the k_entropy loop, each finished block marked ready
@@ -1331,10 +1364,7 @@ __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, 
     __shared__ uint16_t s_bend[9];
     static_assert(sizeof(sA) >= sizeof(uint32_t) * kCtxSlots * 32, "contexts fit in sA");
     const int tid = threadIdx.x;
-    for (int i = tid + 1; i < kN3; i += blockDim.x) {
-        const uint32_t b = scan[i] >> 12;
-        if ((scan[i - 1] >> 12) != b) s_bend[b - 1] = (uint16_t)i;
-    }
+    if (tid < 9) s_bend[tid] = c_bend[tid];
     for (int i = tid; i < 16 * 8; i += blockDim.x) {
         const int k = i >> 3, mm = (i & 7) * 2;
         sW[i] = make_float4(c_cos[k][mm], c_cos[k][mm], c_cos[k][mm + 1], c_cos[k][mm + 1]);
@@ -1342,8 +1372,6 @@ __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, 
     rec_init(sB);
     const uint32_t cap = entry_cap(it.len);
     if (tid == 0) {
-        s_bend[7] = kN3;
-        s_bend[8] = 0xFFFF;
         S->item = it;
         S->base = 0;
         S->pool_used = 0;
@@ -1390,8 +1418,17 @@ __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, 
 }
 
 // ---------------------------------------------------------------- launchers
-cudaError_t upload_cos(const float cmf[16][16], cudaStream_t s) {
-    return cudaMemcpyToSymbolAsync(c_cos, cmf, sizeof(float) * 256, 0, cudaMemcpyHostToDevice, s);
+cudaError_t upload_decode_tables(const float cmf[16][16], const uint16_t scan[kN3], cudaStream_t s) {
+    // pageable sources: the copies are staged before these calls return
+    static uint16_t bend[9];
+    for (int i = 1; i < kN3; ++i) {
+        const uint32_t b = scan[i] >> 12;
+        if ((uint32_t)(scan[i - 1] >> 12) != b) bend[b - 1] = (uint16_t)i;
+    }
+    bend[7] = kN3;
+    bend[8] = 0xFFFF;
+    const cudaError_t e = cudaMemcpyToSymbolAsync(c_cos, cmf, sizeof(float) * 256, 0, cudaMemcpyHostToDevice, s);
+    return e != cudaSuccess ? e : cudaMemcpyToSymbolAsync(c_bend, bend, sizeof bend, 0, cudaMemcpyHostToDevice, s);
 }
 
 static int num_sms() { return dev_sms(); }

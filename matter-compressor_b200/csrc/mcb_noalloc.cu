@@ -157,7 +157,7 @@ int device_scratch(int dev, uint8_t **out) {
         table_scan(scan);
         table_cos(cosm);
         e = cudaMemcpy(static_cast<uint8_t *>(p) + kOffScan, scan, sizeof scan, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = upload_cos(cosm, nullptr);
+        if (e == cudaSuccess) e = upload_decode_tables(cosm, scan, nullptr);
         if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
         if (e != cudaSuccess) return fail(-4, cudaGetErrorString(e));
         ds.scratch = static_cast<uint8_t *>(p);
