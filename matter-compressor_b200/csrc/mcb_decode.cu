@@ -1272,12 +1272,29 @@ __global__ void __launch_bounds__(128, 4) k_decode_fused(FusedParams F) {
     }
     __syncthreads();
 
-    // ---- entropy: the k_entropy loop, each finished block marked ready
+    // ---- entropy: the k_entropy loop, each finished block marked ready;
+    // warps 0..nsolo-1 of the grid first decode order entry `warp` on their
+    // first thread alone, as in k_entropy
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         uint32_t *ctx = &S.u.e.ctx[warp][0][lane];
         LaneState L;
-        run_lanes(L, P, ctx, S.u.e.bend, gtid, nlanes, [&F](int item) { pair_ready(F, item); });
+        const int gwarp = (int)(blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        if (gwarp < P.nsolo) {
+            if (lane == 0) {
+                memset(&L, 0, sizeof L);
+                lane_begin(L, P, ctx, S.u.e.bend, (int)P.order[gwarp]);
+                solo_entropy(L, P, ctx, S.u.e.bend);
+                lane_finish(L, P);
+                pair_ready(F, L.item);
+            }
+            __syncwarp();
+        }
+        EntParams E = P;   // the rest of the order, one lane per block
+        E.order = P.order + P.nsolo;
+        E.ncoded = P.ncoded - P.nsolo;
+        run_lanes(L, E, ctx, S.u.e.bend, gtid - 32 * P.nsolo, nlanes - 32 * P.nsolo,
+                  [&F](int item) { pair_ready(F, item); });
     }
     __syncthreads();   // the shared memory changes hands
     rec_init(S.u.r.B);
@@ -1455,9 +1472,18 @@ static cudaError_t launch_entropy_w(const EntParams &p, int ctas_per_sm, cudaStr
     return cudaGetLastError();
 }
 
+// The single-thread share when a launch configuration leaves it open, from
+// the launch's coded blocks (q=6 batches on a B200): up to about 10 chunks'
+// worth every block on a single thread (its time is the longest block's
+// chain, a few times shorter there), up to about 30 chunks' worth the longest
+// 1/64, beyond that none (a lane of 32 issues fewer instructions per bin).
+constexpr int kSoloAllMax = 28 * 1024, kSoloShareMax = 90 * 1024;
+static int auto_solo(int ncoded) { return ncoded <= kSoloAllMax ? 1 : (ncoded <= kSoloShareMax ? 64 : 0); }
+
 cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_t s) {
     if (p.ncoded <= 0) return cudaSuccess;
-    if (cfg.ent_solo == 1) {   // every block on a single thread
+    const int solo = cfg.ent_solo >= 0 ? cfg.ent_solo : auto_solo(p.ncoded);
+    if (solo == 1) {   // every block on a single thread
         int blocks = (p.ncoded + kSoloWarps - 1) / kSoloWarps;
         if (blocks > 2 * num_sms()) blocks = 2 * num_sms();
         k_entropy_solo<<<blocks, kSoloWarps * 32, 0, s>>>(p);
@@ -1465,7 +1491,7 @@ cudaError_t launch_entropy(const EntParams &p, const LaunchCfg &cfg, cudaStream_
     }
     EntParams q = p;
     q.claim = cfg.ent_claim > 0 ? cfg.ent_claim : 1;
-    q.nsolo = cfg.ent_solo > 0 ? p.ncoded / cfg.ent_solo : 0;
+    q.nsolo = solo > 0 ? p.ncoded / solo : 0;
     const int per_sm = cfg.ent_ctas_per_sm > 0 ? cfg.ent_ctas_per_sm : 5;
     switch (cfg.ent_warps) {
     case 2: return launch_entropy_w<2>(q, per_sm, s);
@@ -1495,7 +1521,12 @@ int fused_grid(const LaunchCfg &cfg) {
 cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_t s) {
     const int blocks = fused_grid(cfg);
     if (blocks <= 0) return cudaErrorInvalidConfiguration;
-    k_decode_fused<<<blocks, 128, sizeof(FusedSmem), s>>>(f);
+    // the single-thread share (all blocks is not a fused layout: at most half
+    // of the warps, as in k_entropy)
+    FusedParams g = f;
+    const int solo = cfg.ent_solo >= 0 ? cfg.ent_solo : auto_solo(f.e.ncoded);
+    g.e.nsolo = solo > 0 ? std::min(f.e.ncoded / solo, blocks * 4 / 2) : 0;
+    k_decode_fused<<<blocks, 128, sizeof(FusedSmem), s>>>(g);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_fused_tail<<<num_sms(), 128, 0, s>>>(f);

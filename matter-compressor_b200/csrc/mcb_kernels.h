@@ -13,9 +13,10 @@ struct LaunchCfg {
     int ent_claim = 1;         // entropy stage: queue entries a lane claims at a time (1, 2 or 4)
     int ent_ctas_per_sm = 5;   // entropy stage: CTAs per SM (8.8 KB of contexts per warp)
     int rec_ctas_per_sm = 4;   // reconstruction stage: CTAs of 128 threads per SM (<= 4: 47 KB smem)
-    int ent_solo = 0;          // entropy stage: the longest ncoded / ent_solo blocks are decoded one per
+    int ent_solo = -1;         // entropy stage: the longest ncoded / ent_solo blocks are decoded one per
                                // warp by a single thread (0: none; see EntParams::nsolo); 1: every
-                               // block, by the single-thread kernel k_entropy_solo
+                               // block, by the single-thread kernel k_entropy_solo; -1: by the
+                               // launch's coded-block count (see launch_entropy)
     bool split = false;        // long blocks on a second stream (batches large enough to split)
     bool fused = false;        // both stages in one persistent kernel (k_decode_fused)
     int fused_ctas_per_sm = 4;

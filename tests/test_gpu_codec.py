@@ -301,15 +301,17 @@ def test_plan_entropy_shapes(gpu, oracle, tmp_path):
             # solo share: 1/16 of the blocks on single-thread warps; 2 asks for
             # more than half of the warps and is clamped to that; 1 is the
             # single-thread kernel
-            for warps, ctas, claim, solo in ((2, 12, 1, 0), (4, 5, 2, 16), (8, 3, 4, 0), (4, 1, 1, 2),
-                                             (2, 3, 64, 1), (4, 5, 1, 64)):
-                assert plan.set_tuning(warps, ctas, claim, 4, "sequential", solo) == 0
+            for warps, ctas, claim, solo, stages in (
+                    (2, 12, 1, 0, "sequential"), (4, 5, 2, 16, "sequential"), (8, 3, 4, 0, "sequential"),
+                    (4, 1, 1, 2, "sequential"), (2, 3, 64, 1, "sequential"), (4, 5, 1, 64, "sequential"),
+                    (4, 5, 1, 1, "long_blocks_on_second_stream"), (4, 5, 1, 8, "fused"), (4, 5, 1, 1, "fused")):
+                assert plan.set_tuning(warps, ctas, claim, 4, stages, solo) == 0
                 assert plan.tuning()["entropy_warps_per_cta"] == warps
                 assert plan.tuning()["entropy_solo_share"] == solo
                 d_out.fill_(0xEE)
                 plan.launch()
                 torch.cuda.synchronize()
-                assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim, solo)
+                assert np.array_equal(d_out.cpu().numpy(), want), (warps, ctas, claim, solo, stages)
             with pytest.raises(RuntimeError, match="bad arguments"):   # 3 warps per CTA: refused
                 plan.set_tuning(3, 4, 1, 4, "sequential")
         finally:
