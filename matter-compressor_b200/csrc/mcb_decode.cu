@@ -1435,6 +1435,20 @@ __global__ void __launch_bounds__(128) k_decode_one(DecItem it, SoloScratch *S, 
 }
 
 // ---------------------------------------------------------------- launchers
+cudaError_t preload_decode_kernels() {
+    // under lazy module loading a kernel's code is loaded at its first launch,
+    // which would put a few milliseconds into the first call that uses it
+    cudaFuncAttributes fa;
+    const void *fns[] = {(const void *)k_entropy<2>, (const void *)k_entropy<4>, (const void *)k_entropy<8>,
+                         (const void *)k_entropy_solo, (const void *)k_reconstruct, (const void *)k_decode_fused,
+                         (const void *)k_fused_tail, (const void *)k_decode_one};
+    for (const void *f : fns) {
+        const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t upload_decode_tables(const float cmf[16][16], const uint16_t scan[kN3], cudaStream_t s) {
     // pageable sources: the copies are staged before these calls return
     static uint16_t bend[9];

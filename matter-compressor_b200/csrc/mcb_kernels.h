@@ -86,6 +86,8 @@ cudaError_t launch_fused(const FusedParams &f, const LaunchCfg &cfg, cudaStream_
 // The decode kernels' constant tables: the cosine basis and the band ends of
 // the scan order (scan position -> raster idx | band << 12).
 cudaError_t upload_decode_tables(const float cmf[16][16], const uint16_t scan[kN3], cudaStream_t s);
+// Loads the decode kernels' code now (first-call latency under lazy loading).
+cudaError_t preload_decode_kernels();
 // Deblocking filter in place on `count` dense nz x ny x nx volumes vstride
 // bytes apart (three stream-ordered kernels: x, y, z faces).
 // LOD pyramid: 2x decimation of a dense dz x dy x dx volume into

@@ -89,7 +89,7 @@ static void runtime_init() {
         cudaMalloc(&R->d_qtab, sizeof(QTab) * kMaxQSlots) != cudaSuccess ||
         cudaMemcpy(R->d_scan, R->h_scan, sizeof R->h_scan, cudaMemcpyHostToDevice) != cudaSuccess ||
         upload_decode_tables(R->h_cos, R->h_scan, 0) != cudaSuccess || upload_cos_encode(R->h_cos, 0) != cudaSuccess ||
-        cudaDeviceSynchronize() != cudaSuccess) {
+        preload_decode_kernels() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
         g_rt_err = std::string("device table upload failed: ") + cudaGetErrorString(cudaGetLastError());
         delete R;
         return;
