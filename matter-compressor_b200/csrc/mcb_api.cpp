@@ -523,16 +523,18 @@ static bool blob_items(const uint8_t *b, uint64_t bl, const uint8_t *d_blob, Dec
 // Host blobs in, host voxels out, as a pipeline of kBlobSlots slots over
 // groups of kBlobGroup chunks: while one slot's voxels travel device->host,
 // the next slots' blobs travel host->device and decode. A slot is reused once
-// the event recorded after its previous group's copy-out has fired; with
-// three slots the host prepares a group while two are still in flight, so a
-// group's decode (about as long as a group's copy-out at 8 chunks) is queued
-// before the link runs dry.
+// the event recorded after its previous group's copy-out has fired. A
+// group's decode takes about its longest block's serial chain, 1.5-1.7 ms at
+// q=6 whatever the group's size, so small groups with many in flight keep the
+// link busy soonest: 2-chunk groups over 8 slots reached 50.5 GB/s for 64
+// chunks where 8-chunk groups over 3 slots gave 49.1 (the plain device-to-host
+// copy on that box: 57.2 GB/s).
 int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens, int n, mc_u8 *out,
                                size_t out_stride) {
     if (n < 0 || (n && (!blobs || !lens || !out))) return -1;
     Lane *L = lane();
     if (!L) return -1;
-    constexpr int kBlobGroup = 8;
+    constexpr int kBlobGroup = 2;
     bool ok = true;
     for (int k = 0; k < kBlobSlots; ++k) ok = ok && blob_slot_ready(L->pipe[k]);
     uint32_t bad = 0;

@@ -94,7 +94,7 @@ struct BlobSlot {
 };
 // Per-thread execution resources: a stream and reusable buffers.
 // Slots of the host-blob decode pipeline (mc_b200_decode_chunk_blobs).
-constexpr int kBlobSlots = 3;
+constexpr int kBlobSlots = 8;
 
 struct Lane {
     cudaStream_t stream = nullptr;
