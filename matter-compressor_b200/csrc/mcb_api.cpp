@@ -79,8 +79,10 @@ bool region_items(mc_archive *a, const uint8_t *dbase, int lod, long z0, long y0
     uint64_t co = 0;
     int slot = 0;
     const ChunkIndex *ix = nullptr;
-    for (long w = 0; w < nbz * nby * nbx; ++w) {
-        const long bz = bz0 + w / (nby * nbx), by = by0 + (w / nbx) % nby, bx = bx0 + w % nbx;
+    if (nbz > 0 && nby > 0 && nbx > 0) items.reserve(items.size() + (size_t)(nbz * nby * nbx));
+    for (long bz = bz0; bz < bz0 + nbz; ++bz)
+    for (long by = by0; by < by0 + nby; ++by)
+    for (long bx = bx0; bx < bx0 + nbx; ++bx) {
         const long gz = bz * 16, gy = by * 16, gx = bx * 16;
         const long iz0 = std::max(gz, z0), iz1 = std::min(gz + 16, z0 + dz);
         const long iy0 = std::max(gy, y0), iy1 = std::min(gy + 16, y0 + dy);
@@ -437,6 +439,8 @@ int mc_b200_read_regions_dev(mc_archive *a, int lod, const mc_box *boxes, int n,
     if (!dbase) return -1;
     if (s != L->stream && !cuda_ok(cudaStreamWaitEvent(s, a->mir_ev, 0), "stream wait")) return -1;
     std::vector<DecItem> items;
+    // at most this many blocks per box (an unaligned box touches one more per axis)
+    items.reserve((size_t)n * (size_t)((dz + 31) >> 4) * (size_t)((dy + 31) >> 4) * (size_t)((dx + 31) >> 4));
     for (int i = 0; i < n; ++i)
         if (!region_items(a, dbase, lod, boxes[i].z0, boxes[i].y0, boxes[i].x0, dz, dy, dx,
                           d_out + (size_t)i * batch_stride, (int64_t)dy * dx, dx, items))

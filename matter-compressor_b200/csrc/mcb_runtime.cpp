@@ -387,7 +387,13 @@ bool decode_items(Lane &L, const DecItem *items, int n, cudaStream_t s) {
     if (n <= 0) return true;
     if (!s) s = L.stream;
     if (!cuda_ok(cudaEventSynchronize(L.done), "event sync")) return false;
-    if (!decode_prepare(L.batch, items, n, s) || !decode_enqueue(L.batch, L.cfg, s)) return false;
+    // the items go to the lane's pinned staging (the caller's array may be
+    // pageable and short-lived), then every upload is asynchronous; the
+    // staging is reused only after L.done, recorded behind this batch
+    DecodeBatch &B = L.batch;
+    if (!B.h_items.ensure(sizeof(DecItem) * (size_t)n)) return false;
+    memcpy(B.h_items.p, items, sizeof(DecItem) * (size_t)n);
+    if (!decode_prepare_staged(B, n, s) || !decode_enqueue(B, L.cfg, s)) return false;
     return cuda_ok(cudaEventRecord(L.done, s), "event record");
 }
 
