@@ -141,6 +141,18 @@ void mc_b200_clear_error(void);
 /* Blocks of the calling thread's last decode whose corrupt stream was cut
  * short (Exp-Golomb prefix cap or overflow-pool exhaustion). */
 uint32_t mc_b200_last_bad_blocks(void);
+/* How the calling thread's decodes without a plan (per-call chunk, block and
+ * region reads, the host-blob pipeline) split the entropy stage between its
+ * two kernels. A lane of a warp decodes a block at about 5 issue slots per
+ * bin but about 450 cycles per bin; one thread alone takes about 25 slots but
+ * about 120 cycles. share > 1: the longest coded/share blocks on single
+ * threads, the rest one per lane; 1: every block on a single thread; 0: every
+ * block on a lane; -1 (the default): by the launch's coded-block count (every
+ * block on single threads up to 28 K blocks, the longest 1/64 up to 90 K), and
+ * lanes only in the host-blob pipeline, whose groups overlap. Decoded voxels
+ * are the same in every case. 0, or -1 for share < -1. No reference
+ * counterpart. */
+int  mc_b200_set_entropy_solo(int share);
 
 /* Decode n whole chunk blobs held in HOST memory (blob i: blobs[i], blob_lens[i]
  * bytes, as stored in an archive) into HOST memory, chunk i at

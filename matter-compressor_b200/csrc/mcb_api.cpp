@@ -296,6 +296,16 @@ int mc_b200_device(void) {
 }
 const char *mc_b200_last_error(void) { return last_error(); }
 void mc_b200_clear_error(void) { clear_error(); }
+int mc_b200_set_entropy_solo(int share) {
+    if (share < -1) {
+        set_error("set_entropy_solo: bad arguments");
+        return -1;
+    }
+    Lane *L = lane();
+    if (!L) return -1;
+    L->cfg.ent_solo = share;
+    return 0;
+}
 uint32_t mc_b200_last_bad_blocks(void) {
     Lane *L = lane();
     return L ? lane_bad_blocks(*L) : 0;

@@ -102,6 +102,7 @@ class McLib:
                 "mc_b200_last_error": (C.c_char_p, []),
                 "mc_b200_clear_error": (None, []),
                 "mc_b200_last_bad_blocks": (u32, []),
+                "mc_b200_set_entropy_solo": (i, [i]),
                 "mc_b200_decode_chunk_blobs": (i, [vp, vp, i, u8p, sz]),
                 "mc_b200_archive_sync": (i, [vp, C.POINTER(C.c_void_p), C.POINTER(u64)]),
                 "mc_b200_decode_chunks_dev": (i, [vp, vp, i, vp, sz, vp]),

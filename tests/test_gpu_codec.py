@@ -47,6 +47,49 @@ def test_corrupt_streams_golden(gpu, golden_corrupt):
     assert gpu.L.mc_b200_last_bad_blocks() == 0
 
 
+def _blob_of(payloads, q):
+    """A chunk blob whose blocks 0..n-1 carry the given payloads (no fracmap,
+    hash 0: the decode reads neither)."""
+    bm = np.zeros(512, np.uint8)
+    for i in range(len(payloads)):
+        bm[i >> 3] |= 1 << (i & 7)
+    lens = np.asarray([len(p) for p in payloads], np.uint16)
+    head = np.float32(q).tobytes() + bytes(8) + np.uint16(0).tobytes()
+    return np.frombuffer(head + bm.tobytes() + lens.tobytes() + b"".join(payloads), np.uint8)
+
+
+def test_corrupt_streams_every_entropy_kernel(gpu, golden_corrupt):
+    """The corrupt-stream corpus decoded as blocks of chunk blobs by each way
+    of running the entropy stage: one block per lane of a warp, every block on
+    a single thread, and the longest eighth on single threads with the rest on
+    lanes. Every block equals the reference's decode of its stream."""
+    import ctypes as C
+    g = golden_corrupt
+    groups = {}
+    for i in range(len(g["q"])):
+        groups.setdefault(float(g["q"][i]), []).append(i)
+    blobs, want = [], []
+    for q, idx in sorted(groups.items()):
+        blobs.append(_blob_of([g["payload"][g["offs"][i]:g["offs"][i + 1]].tobytes() for i in idx], q))
+        want.append([str(g["decoded_sha"][i]) for i in idx])
+    ptrs = (C.c_void_p * len(blobs))(*[b.ctypes.data for b in blobs])
+    lens = np.asarray([b.size for b in blobs], np.uint64)
+    try:
+        for share in (0, 1, 8):
+            assert gpu.L.mc_b200_set_entropy_solo(share) == 0
+            out = np.zeros(len(blobs) * CHUNK, np.uint8)
+            assert gpu.L.mc_b200_decode_chunk_blobs(C.cast(ptrs, C.c_void_p), lens.ctypes.data, len(blobs),
+                                                    out.ctypes.data, CHUNK) == 0
+            for c, shas in enumerate(want):
+                vol = out[c * CHUNK:(c + 1) * CHUNK].reshape(256, 256, 256)
+                for bi, h in enumerate(shas):
+                    bz, by, bx = bi >> 8, (bi >> 4) & 15, bi & 15
+                    blk = np.ascontiguousarray(vol[bz * 16:bz * 16 + 16, by * 16:by * 16 + 16, bx * 16:bx * 16 + 16])
+                    assert sha(blk) == h, (share, c, bi)
+    finally:
+        gpu.L.mc_b200_set_entropy_solo(-1)
+
+
 def test_chunk_blobs_decode_golden(gpu, golden_chunks):
     from mcb200 import decode_chunk_blobs
     g = golden_chunks
@@ -57,9 +100,9 @@ def test_chunk_blobs_decode_golden(gpu, golden_chunks):
 
 
 def test_chunk_blobs_pipeline(gpu, golden_chunks):
-    """More blobs than the pipeline has slots (five groups of up to 8 over
-    three slots, so two slots are reused), a missing blob, and a padded output
-    stride: every chunk still matches."""
+    """More blobs than the pipeline has slots (18 groups of up to 2 over 8
+    slots, so slots are reused), a missing blob, and a padded output stride:
+    every chunk still matches."""
     import ctypes as C
     g = golden_chunks
     blobs = [g["blobs"][g["offs"][i]:g["offs"][i + 1]] for i in range(len(g["offs"]) - 1)]
