@@ -68,56 +68,54 @@ void zero_chunk_items(uint8_t *d_chunk_out, DecItem *items) {
 
 // Items for one region of `lod` (src/mc_archive.c:984-1042): every touched
 // block contributes its intersection with the region; voxel (z,y,x) of the
-// region lands at d_origin + z*sz + y*sy + x.
+// region lands at d_origin + z*sz + y*sy + x. The blocks are walked chunk by
+// chunk, so each touched chunk's block index is looked up once per region
+// (a box crosses up to 8 chunks, whose indexes may share a slot of the
+// per-thread index cache).
 bool region_items(mc_archive *a, const uint8_t *dbase, int lod, long z0, long y0, long x0, long dz, long dy,
                   long dx, uint8_t *d_origin, int64_t sz, int64_t sy, std::vector<DecItem> &items) {
     const long bz0 = z0 >> 4, by0 = y0 >> 4, bx0 = x0 >> 4;
-    const long nbz = ((z0 + dz + 15) >> 4) - bz0, nby = ((y0 + dy + 15) >> 4) - by0,
-               nbx = ((x0 + dx + 15) >> 4) - bx0;
+    const long bz1 = (z0 + dz + 15) >> 4, by1 = (y0 + dy + 15) >> 4, bx1 = (x0 + dx + 15) >> 4;   // exclusive
+    if (bz1 <= bz0 || by1 <= by0 || bx1 <= bx0) return true;
+    items.reserve(items.size() + (size_t)((bz1 - bz0) * (by1 - by0) * (bx1 - bx0)));
     const uint64_t cur = a->cursor.load(std::memory_order_acquire);
-    long last_cz = -1, last_cy = -1, last_cx = -1;
-    uint64_t co = 0;
-    int slot = 0;
-    const ChunkIndex *ix = nullptr;
-    if (nbz > 0 && nby > 0 && nbx > 0) items.reserve(items.size() + (size_t)(nbz * nby * nbx));
-    for (long bz = bz0; bz < bz0 + nbz; ++bz)
-    for (long by = by0; by < by0 + nby; ++by)
-    for (long bx = bx0; bx < bx0 + nbx; ++bx) {
-        const long gz = bz * 16, gy = by * 16, gx = bx * 16;
-        const long iz0 = std::max(gz, z0), iz1 = std::min(gz + 16, z0 + dz);
-        const long iy0 = std::max(gy, y0), iy1 = std::min(gy + 16, y0 + dy);
-        const long ix0 = std::max(gx, x0), ix1 = std::min(gx + 16, x0 + dx);
-        if (iz0 >= iz1 || iy0 >= iy1 || ix0 >= ix1) continue;
-        const long cz = bz >> 4, cy = by >> 4, cx = bx >> 4;
-        if (cz != last_cz || cy != last_cy || cx != last_cx) {
-            co = mc_archive_chunk_offset(a, lod, (int)cz, (int)cy, (int)cx);
-            last_cz = cz; last_cy = cy; last_cx = cx;
-            ix = nullptr;
-            if (co > kSlotZero) {
-                slot = qslot(sanitize_q(chunk_q(a, co)));
-                if (slot < 0) return false;
-                ix = &chunk_index(a->base, co);
-            }
+    for (long cz = bz0 >> 4; cz <= (bz1 - 1) >> 4; ++cz)
+    for (long cy = by0 >> 4; cy <= (by1 - 1) >> 4; ++cy)
+    for (long cx = bx0 >> 4; cx <= (bx1 - 1) >> 4; ++cx) {
+        const uint64_t co = mc_archive_chunk_offset(a, lod, (int)cz, (int)cy, (int)cx);
+        int slot = 0;
+        const ChunkIndex *ix = nullptr;
+        if (co > kSlotZero) {
+            slot = qslot(sanitize_q(chunk_q(a, co)));
+            if (slot < 0) return false;
+            ix = &chunk_index(a->base, co);   // nothing below rebuilds another index
         }
-        DecItem it;
-        memset(&it, 0, sizeof it);
-        if (ix) {
-            // re-fetch: the thread-local index may have been rebuilt for another chunk
-            ix = &chunk_index(a->base, co);
-            const int bi = (int)(((bz & 15) * 16 + (by & 15)) * 16 + (bx & 15));
-            const uint64_t off = ix->off[bi];
-            if (off && off + ix->len[bi] <= cur) {
-                it.src = dptr(dbase + off);
-                it.len = ix->len[bi];
+        for (long bz = std::max(bz0, cz * 16); bz < std::min(bz1, cz * 16 + 16); ++bz)
+        for (long by = std::max(by0, cy * 16); by < std::min(by1, cy * 16 + 16); ++by)
+        for (long bx = std::max(bx0, cx * 16); bx < std::min(bx1, cx * 16 + 16); ++bx) {
+            const long gz = bz * 16, gy = by * 16, gx = bx * 16;
+            const long iz0 = std::max(gz, z0), iz1 = std::min(gz + 16, z0 + dz);
+            const long iy0 = std::max(gy, y0), iy1 = std::min(gy + 16, y0 + dy);
+            const long ix0 = std::max(gx, x0), ix1 = std::min(gx + 16, x0 + dx);
+            if (iz0 >= iz1 || iy0 >= iy1 || ix0 >= ix1) continue;
+            DecItem it;
+            memset(&it, 0, sizeof it);
+            if (ix) {
+                const int bi = (int)(((bz & 15) * 16 + (by & 15)) * 16 + (bx & 15));
+                const uint64_t off = ix->off[bi];
+                if (off && off + ix->len[bi] <= cur) {
+                    it.src = dptr(dbase + off);
+                    it.len = ix->len[bi];
+                }
             }
+            it.dst = dptr(d_origin + (gz - z0) * sz + (gy - y0) * sy + (gx - x0));
+            it.sz = sz;
+            it.sy = sy;
+            it.qslot = (uint16_t)slot;
+            it.clip_lo = (uint16_t)(((iz0 - gz) << 8) | ((iy0 - gy) << 4) | (ix0 - gx));
+            it.clip_hi = (uint16_t)(((iz1 - 1 - gz) << 8) | ((iy1 - 1 - gy) << 4) | (ix1 - 1 - gx));
+            items.push_back(it);
         }
-        it.dst = dptr(d_origin + (gz - z0) * sz + (gy - y0) * sy + (gx - x0));
-        it.sz = sz;
-        it.sy = sy;
-        it.qslot = (uint16_t)slot;
-        it.clip_lo = (uint16_t)(((iz0 - gz) << 8) | ((iy0 - gy) << 4) | (ix0 - gx));
-        it.clip_hi = (uint16_t)(((iz1 - 1 - gz) << 8) | ((iy1 - 1 - gy) << 4) | (ix1 - 1 - gx));
-        items.push_back(it);
     }
     return true;
 }
