@@ -345,9 +345,7 @@ void mc_archive_decode_chunk(mc_archive *a, uint64_t co, mc_u8 *out, int nthread
     if (!dbase || !L->out.ensure(kChunkBytes)) { memset(out, 0, kChunkBytes); return; }
     std::vector<DecItem> items(kGrid3);
     chunk_items(a, co, dbase, slot, L->out.as<uint8_t>(), items.data());
-    if (!decode_items(*L, items.data(), kGrid3) ||
-        !cuda_ok(cudaMemcpyAsync(out, L->out.p, kChunkBytes, cudaMemcpyDeviceToHost, L->stream), "D2H") ||
-        !finish(*L, nullptr))
+    if (!decode_items(*L, items.data(), kGrid3) || !copy_to_host(*L, out, L->out.as<uint8_t>(), kChunkBytes))
         memset(out, 0, kChunkBytes);
 }
 
@@ -366,13 +364,13 @@ void mc_archive_read_region(mc_archive *a, int lod, long z0, long y0, long x0, l
     if (!decode_items(*L, items.data(), (int)items.size())) return;
     bool ok = true;
     if (sy == (size_t)dx && sz == (size_t)dy * dx) {
-        ok = cuda_ok(cudaMemcpyAsync(out, L->out.p, dense, cudaMemcpyDeviceToHost, L->stream), "D2H");
-    } else {
-        for (long z = 0; z < dz && ok; ++z)
-            ok = cuda_ok(cudaMemcpy2DAsync(out + z * sz, sy, L->out.as<uint8_t>() + (size_t)z * dy * dx, dx, dx, dy,
-                                           cudaMemcpyDeviceToHost, L->stream),
-                         "D2H");
+        copy_to_host(*L, out, L->out.as<uint8_t>(), dense);
+        return;
     }
+    for (long z = 0; z < dz && ok; ++z)
+        ok = cuda_ok(cudaMemcpy2DAsync(out + z * sz, sy, L->out.as<uint8_t>() + (size_t)z * dy * dx, dx, dx, dy,
+                                       cudaMemcpyDeviceToHost, L->stream),
+                     "D2H");
     if (ok) finish(*L, nullptr);
 }
 
@@ -392,16 +390,7 @@ void mc_archive_read_regions(mc_archive *a, int lod, const mc_box *boxes, int n,
                           L->out.as<uint8_t>() + crop * i, (int64_t)dy * dx, dx, items))
             return;
     if (!decode_items(*L, items.data(), (int)items.size())) return;
-    bool ok = true;
-    if (batch_stride == crop) {
-        ok = cuda_ok(cudaMemcpyAsync(out, L->out.p, crop * n, cudaMemcpyDeviceToHost, L->stream), "D2H");
-    } else {
-        for (int i = 0; i < n && ok; ++i)
-            ok = cuda_ok(cudaMemcpyAsync(out + (size_t)i * batch_stride, L->out.as<uint8_t>() + crop * i, crop,
-                                         cudaMemcpyDeviceToHost, L->stream),
-                         "D2H");
-    }
-    if (ok) finish(*L, nullptr);
+    copy_to_host(*L, out, L->out.as<uint8_t>(), crop * n, crop, batch_stride);
 }
 
 // ============================================================ device-output decode

@@ -5,6 +5,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <thread>
 
 #include "mcb_tables.h"
 
@@ -138,8 +141,151 @@ float slot_quality(int slot) {
 
 // ------------------------------------------------------------------ lanes
 Lane::~Lane() {
+    for (cudaEvent_t e : bounce_ev)
+        if (e) cudaEventDestroy(e);
     if (done) cudaEventDestroy(done);
     if (stream) cudaStreamDestroy(stream);
+}
+
+// ------------------------------------------------------------- host copies
+// A few host threads that split large memcpys into stripes; the calling
+// thread takes stripes too. One job at a time (calls from several host
+// threads queue on the pool's lock).
+namespace {
+struct CopyPool {
+    std::mutex run_mu;                 // one job at a time
+    std::mutex mu;                     // guards the job's fields, gen, active, stop
+    std::condition_variable cv, done_cv;
+    std::vector<std::thread> workers;
+    uint8_t *dst = nullptr;
+    const uint8_t *src = nullptr;
+    size_t n = 0, stripe = 0;
+    std::atomic<size_t> next{0}, left{0};
+    uint64_t gen = 0;
+    int active = 0;                    // workers inside a job's stripes
+    bool stop = false;
+
+    // Stripes of the current job until none is left; the fields were read
+    // under mu by the caller of work().
+    void work(uint8_t *d, const uint8_t *s_, size_t bytes, size_t st) {
+        for (;;) {
+            const size_t off = next.fetch_add(1) * st;
+            if (off >= bytes) return;
+            memcpy(d + off, s_ + off, std::min(st, bytes - off));
+            if (left.fetch_sub(1) == 1) {
+                std::lock_guard<std::mutex> g(mu);
+                done_cv.notify_all();
+            }
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            uint8_t *d;
+            const uint8_t *s_;
+            size_t bytes, st;
+            {
+                std::unique_lock<std::mutex> g(mu);
+                cv.wait(g, [&] { return stop || gen != seen; });
+                if (stop) return;
+                seen = gen;
+                ++active;
+                d = dst; s_ = src; bytes = n; st = stripe;
+            }
+            work(d, s_, bytes, st);
+            {
+                std::lock_guard<std::mutex> g(mu);
+                --active;
+            }
+            done_cv.notify_all();
+        }
+    }
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned t = std::min(7u, hw > 2 ? hw / 2 : 1u);
+        for (unsigned i = 0; i < t; ++i) workers.emplace_back([this] { loop(); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        for (auto &w : workers) w.join();
+    }
+    void copy(uint8_t *d, const uint8_t *s_, size_t bytes) {
+        constexpr size_t kStripe = 256u << 10;   // a 2 MiB segment still spreads over 8 threads
+        if (bytes < 2 * kStripe || workers.empty()) {
+            memcpy(d, s_, bytes);
+            return;
+        }
+        std::lock_guard<std::mutex> r(run_mu);
+        {
+            // no worker is still inside the previous job when its counters reset
+            std::unique_lock<std::mutex> g(mu);
+            done_cv.wait(g, [&] { return active == 0; });
+            dst = d; src = s_; n = bytes; stripe = kStripe;
+            left.store((bytes + kStripe - 1) / kStripe);
+            next.store(0);
+            ++gen;
+        }
+        cv.notify_all();
+        work(d, s_, bytes, kStripe);
+        std::unique_lock<std::mutex> g(mu);
+        done_cv.wait(g, [&] { return left.load() == 0; });
+    }
+};
+CopyPool &copy_pool() {
+    static CopyPool pool;
+    return pool;
+}
+}  // namespace
+
+bool copy_to_host(Lane &L, uint8_t *dst, const uint8_t *d_src, size_t n, size_t seg, size_t dst_stride) {
+    if (seg == 0 || seg > n) seg = n;
+    if (dst_stride == 0) dst_stride = seg;
+    if (n == 0) return cuda_ok(cudaStreamSynchronize(L.stream), "sync");
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, dst) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();   // a pageable pointer may leave an error behind on older drivers
+    constexpr size_t kPiece = 8u << 20;
+    if (pinned || n <= kPiece) {
+        // pinned: the link's rate directly; small: one pageable copy per segment
+        bool ok = true;
+        for (size_t o = 0; o < n && ok; o += seg)
+            ok = cuda_ok(cudaMemcpyAsync(dst + (o / seg) * dst_stride, d_src + o, std::min(seg, n - o),
+                                         cudaMemcpyDeviceToHost, L.stream), "D2H");
+        return cuda_ok(cudaStreamSynchronize(L.stream), "sync") && ok;
+    }
+    constexpr int K = 3;
+    for (int k = 0; k < K; ++k)
+        if (!L.h_bounce[k].ensure(kPiece) ||
+            (!L.bounce_ev[k] && !cuda_ok(cudaEventCreateWithFlags(&L.bounce_ev[k], cudaEventDisableTiming), "event")))
+            return false;
+    const size_t pieces = (n + kPiece - 1) / kPiece;
+    auto len_of = [&](size_t i) { return std::min(kPiece, n - i * kPiece); };
+    auto enqueue = [&](size_t i) {
+        return cuda_ok(cudaMemcpyAsync(L.h_bounce[i % K].p, d_src + i * kPiece, len_of(i), cudaMemcpyDeviceToHost,
+                                       L.stream), "D2H") &&
+               cuda_ok(cudaEventRecord(L.bounce_ev[i % K], L.stream), "event record");
+    };
+    bool ok = true;
+    for (size_t i = 0; i < std::min<size_t>(K, pieces) && ok; ++i) ok = enqueue(i);
+    for (size_t j = 0; j < pieces && ok; ++j) {
+        ok = cuda_ok(cudaEventSynchronize(L.bounce_ev[j % K]), "event sync");
+        if (!ok) break;
+        // the piece's bytes [o, o + len) of the device range, split at segment ends
+        const uint8_t *b = L.h_bounce[j % K].as<uint8_t>();
+        const size_t o0 = j * kPiece, o1 = o0 + len_of(j);
+        for (size_t o = o0; o < o1;) {
+            const size_t e = std::min(o1, (o / seg + 1) * seg);
+            copy_pool().copy(dst + (o / seg) * dst_stride + o % seg, b + (o - o0), e - o);
+            o = e;
+        }
+        if (j + K < pieces) ok = enqueue(j + K);   // buffer j % K is free again
+    }
+    // nothing of this call may still be in flight when it returns
+    return cuda_ok(cudaStreamSynchronize(L.stream), "sync") && ok;
 }
 
 static thread_local Lane *t_lane = nullptr;

@@ -110,6 +110,8 @@ struct Lane {
     DevBuf solo;                                // single-block decode scratch (SoloScratch)
     HostBuf h_items, h_base, h_stage, h_misc;
     HostBuf h_one;                              // single-block output, written by the kernel over the bus
+    HostBuf h_bounce[3];                        // device-to-host pieces bound for pageable memory
+    cudaEvent_t bounce_ev[3] = {};
     LaunchCfg cfg;
     BlobSlot pipe[kBlobSlots];
     ~Lane();
@@ -127,6 +129,15 @@ bool blob_slot_ready(BlobSlot &S);
 bool decode_enqueue(DecodeBatch &B, const LaunchCfg &cfg, cudaStream_t s);
 // One stage only: 0 = status reset + entropy, 1 = reconstruction.
 bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaStream_t s);
+
+// Copies n bytes of device memory to host memory dst after the work already
+// on the lane's stream, and returns when they are there. A dst in pageable
+// memory takes pinned bounce buffers: 8 MiB pieces travel while earlier ones
+// are copied out by host threads, so the copy runs near the link's rate
+// instead of the driver's pageable path (about 3 GB/s here). False on a CUDA
+// error. With seg > 0 the device range is n / seg segments of seg bytes,
+// segment k bound for dst + k * dst_stride.
+bool copy_to_host(Lane &L, uint8_t *dst, const uint8_t *d_src, size_t n, size_t seg = 0, size_t dst_stride = 0);
 
 // Decodes n items whose src/dst are device addresses (host-side item array),
 // enqueued on stream s (null: the lane's stream); false on a launch error.
