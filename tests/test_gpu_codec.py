@@ -361,6 +361,36 @@ def test_plan_entropy_shapes(gpu, oracle, tmp_path):
             plan.free()
 
 
+def test_host_region_batch_through_bounce_buffers(gpu, tmp_path):
+    """A host-output region batch larger than one pinned bounce piece (crops
+    of 3.1 MB, a stride with a gap, about 22 MB in all, so crops straddle the
+    8 MiB pieces) equals the device-output batch crop for crop, twice in a
+    row, and leaves the gaps between crops as they were."""
+    import ctypes as C
+    import torch
+    from mcb200 import McBox
+    with gpu.open(str(tmp_path / "hb.mca"), 1024, 1024, 1024, 6.0) as a:
+        for st in shapes.archive_sequence()[:2]:
+            assert a.append_par(0, *st["at"], shapes.chunk_source(st["src"]), st["q"]) == 0
+        boxes = [(0, 0, 0), (10, 20, 30), (60, 100, 200), (64, 64, 300), (-8, 250, 1000), (200, 200, 450),
+                 (100, 0, 0)]
+        dz, dy, dx = 96, 160, 200
+        crop = dz * dy * dx
+        stride = crop + 4099
+        want = torch.zeros(stride * len(boxes), dtype=torch.uint8, device="cuda")
+        assert a.read_regions_dev(0, boxes, dz, dy, dx, want.data_ptr(), stride) == 0
+        w = want.cpu().numpy()
+        arr = (McBox * len(boxes))(*[McBox(*b) for b in boxes])
+        host = np.full(stride * (len(boxes) - 1) + crop, 0xA5, np.uint8)
+        for _ in range(2):
+            a.L.mc_archive_read_regions(a.a, 0, C.cast(arr, C.c_void_p), len(boxes), dz, dy, dx,
+                                        host.ctypes.data, stride, 0)
+            for i in range(len(boxes)):
+                assert np.array_equal(host[i * stride:i * stride + crop], w[i * stride:i * stride + crop]), boxes[i]
+                if i + 1 < len(boxes):
+                    assert np.all(host[i * stride + crop:(i + 1) * stride] == 0xA5)
+
+
 def test_region_plan(gpu, tmp_path):
     """A graph-captured plan of a region batch (boxes across chunk borders,
     into absent chunks and past the volume, strided output) gives what
