@@ -156,6 +156,20 @@ int mark_zero(mc_archive *a, int lod, int cz, int cy, int cx) {
     a->gen.fetch_add(1, std::memory_order_release);
     return 0;
 }
+// Bytes into the file at off, seen through the shared mapping at once (one
+// page cache): pwrite fills the pages without a fault per page of the
+// mapping, which a memcpy into freshly allocated file pages takes.
+static void write_file(mc_archive *a, uint64_t off, const uint8_t *src, size_t len) {
+    size_t done = 0;
+    while (done < len) {
+        const ssize_t w = pwrite(a->fd, src + done, len - done, (off_t)(off + done));
+        if (w < 0 && errno == EINTR) continue;
+        if (w <= 0) break;
+        done += (size_t)w;
+    }
+    if (done < len) memcpy(a->base + off + done, src + done, len - done);
+}
+
 // src/mc_archive.c:458-485
 int install_blob(mc_archive *a, int lod, int cz, int cy, int cx, const uint8_t *blob, size_t len) {
     std::lock_guard<std::mutex> g(a->write_mu);
@@ -163,7 +177,7 @@ int install_blob(mc_archive *a, int lod, int cz, int cy, int cx, const uint8_t *
     if (slot == ~0ull) return -1;
     uint64_t off = alloc_at_eof(a, len);
     if (off == ~0ull) return -1;
-    memcpy(a->base + off, blob, len);
+    write_file(a, off, blob, len);
     slot_at(a, slot)->store(off, std::memory_order_release);
     touch(a, slot, 8);
     a->gen.fetch_add(1, std::memory_order_release);
