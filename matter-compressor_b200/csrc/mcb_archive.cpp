@@ -297,9 +297,7 @@ uint8_t *mirror_sync(mc_archive *a, Lane &L) {
     }
     a->dirty.clear();
     if (cur > a->synced) {
-        if (!cuda_ok(cudaMemcpyAsync(a->d_base + a->synced, a->base + a->synced, cur - a->synced,
-                                     cudaMemcpyHostToDevice, L.stream), "mirror sync"))
-            return nullptr;
+        if (!copy_to_device(L, a->d_base + a->synced, a->base + a->synced, cur - a->synced)) return nullptr;
         a->synced = cur;
         copied = true;
     }

@@ -288,6 +288,32 @@ bool copy_to_host(Lane &L, uint8_t *dst, const uint8_t *d_src, size_t n, size_t 
     return cuda_ok(cudaStreamSynchronize(L.stream), "sync") && ok;
 }
 
+bool copy_to_device(Lane &L, uint8_t *d_dst, const uint8_t *src, size_t n) {
+    constexpr size_t kPiece = 8u << 20;
+    if (n <= kPiece)
+        return cuda_ok(cudaMemcpyAsync(d_dst, src, n, cudaMemcpyHostToDevice, L.stream), "H2D");
+    constexpr int K = 3;
+    for (int k = 0; k < K; ++k)
+        if (!L.h_bounce[k].ensure(kPiece) ||
+            (!L.bounce_ev[k] && !cuda_ok(cudaEventCreateWithFlags(&L.bounce_ev[k], cudaEventDisableTiming), "event")))
+            return false;
+    const size_t pieces = (n + kPiece - 1) / kPiece;
+    bool ok = true;
+    for (size_t i = 0; i < pieces && ok; ++i) {
+        const int k = (int)(i % K);
+        const size_t len = std::min(kPiece, n - i * kPiece);
+        // the buffer's previous piece (of this call or an earlier one) has left
+        // it; an event never recorded counts as done
+        ok = cuda_ok(cudaEventSynchronize(L.bounce_ev[k]), "event sync");
+        if (!ok) break;
+        copy_pool().copy(L.h_bounce[k].as<uint8_t>(), src + i * kPiece, len);
+        ok = cuda_ok(cudaMemcpyAsync(d_dst + i * kPiece, L.h_bounce[k].p, len, cudaMemcpyHostToDevice, L.stream),
+                     "H2D") &&
+             cuda_ok(cudaEventRecord(L.bounce_ev[k], L.stream), "event record");
+    }
+    return ok;
+}
+
 static thread_local Lane *t_lane = nullptr;
 static thread_local struct LaneOwner { ~LaneOwner() { delete t_lane; t_lane = nullptr; } } t_lane_owner;
 

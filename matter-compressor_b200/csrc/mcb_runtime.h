@@ -138,6 +138,12 @@ bool decode_enqueue_stage(DecodeBatch &B, const LaunchCfg &cfg, int stage, cudaS
 // error. With seg > 0 the device range is n / seg segments of seg bytes,
 // segment k bound for dst + k * dst_stride.
 bool copy_to_host(Lane &L, uint8_t *dst, const uint8_t *d_src, size_t n, size_t seg = 0, size_t dst_stride = 0);
+// The other direction, for large ranges of pageable host memory (a mapped
+// archive file): host threads fill 8 MiB pinned pieces while earlier pieces
+// cross the link. The copies are enqueued on the lane's stream; the call
+// returns once the last piece has been handed to the stream, so later work
+// on the stream sees the bytes. False on a CUDA error.
+bool copy_to_device(Lane &L, uint8_t *d_dst, const uint8_t *src, size_t n);
 
 // Decodes n items whose src/dst are device addresses (host-side item array),
 // enqueued on stream s (null: the lane's stream); false on a launch error.
