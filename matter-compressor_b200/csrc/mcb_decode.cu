@@ -806,12 +806,31 @@ __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); 
 // sequential sum over ascending k (src/mc_codec_float.h:102-104). in[k*ks]
 // holds the 4 lines' k-th inputs, W[k*16 + m/2] = {c[k][m], c[k][m], c[k][m+1], c[k][m+1]}.
 struct Acc4 { float2 e0a, e0b, e1a, e1b, o0a, o0b, o1a, o1b; };
+// From four terms on, each sum starts from its first product rather than
+// from 0 plus it: equal, except that 0 + (-0) is +0 where the product alone
+// keeps -0; a zero of either sign stays a zero through every later add and
+// multiply and rounds to the same voxel, and every nonzero sum is unchanged.
+// With fewer terms a half-sum could be a bare product, which the packed e +/- o
+// below would take into one fused rounding (see madd2), so those start at 0.
 __device__ __forceinline__ Acc4 lines4(const float4 *in, int ks, int K, const float4 *W, int mh) {
     Acc4 a;
-    const float2 z = make_float2(0.f, 0.f);
-    a.e0a = a.e0b = a.e1a = a.e1b = a.o0a = a.o0b = a.o1a = a.o1b = z;
+    int k;
+    if (K >= 4) {
+        const float4 v = in[0], w = W[mh];
+        const float2 w0 = lo2(w), w1 = hi2(w);
+        a.e0a = mul2(w0, lo2(v)); a.e0b = mul2(w0, hi2(v));
+        a.e1a = mul2(w1, lo2(v)); a.e1b = mul2(w1, hi2(v));
+        const float4 u = in[ks], x = W[8 + mh];
+        const float2 x0 = lo2(x), x1 = hi2(x);
+        a.o0a = mul2(x0, lo2(u)); a.o0b = mul2(x0, hi2(u));
+        a.o1a = mul2(x1, lo2(u)); a.o1b = mul2(x1, hi2(u));
+        k = 2;
+    } else {
+        const float2 z = make_float2(0.f, 0.f);
+        a.e0a = a.e0b = a.e1a = a.e1b = a.o0a = a.o0b = a.o1a = a.o1b = z;
+        k = 0;
+    }
     // (even, odd) pairs of k without a per-step guard, then the last even k
-    int k = 0;
 #pragma unroll 2
     for (; k + 1 < K; k += 2) {
         const float4 v = in[k * ks], w = W[k * 8 + mh];
