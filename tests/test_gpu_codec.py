@@ -143,6 +143,40 @@ def test_archive_byte_identical(gpu, golden_chunks, tmp_path):
     assert hashlib.sha256(data).hexdigest() == str(g["archive_sha"])
 
 
+def test_host_output_calls_from_threads(gpu, golden_chunks, tmp_path):
+    """Four host threads decode the archive's chunks into their own pageable
+    buffers at the same time, three rounds each: every thread has its own
+    stream and pinned bounce buffers, and all of them share one pool of host
+    copy threads. Every chunk matches its golden digest."""
+    import threading
+    g = golden_chunks
+    path = str(tmp_path / "t.mca")
+    _, offs = _append_sequence(gpu, path)
+    errors = []
+    with gpu.open(path, 1024, 1024, 1024, 6.0) as a:
+        a.decode_chunk(offs[0])   # the archive's device mirror, before the threads start
+
+        def worker(t):
+            try:
+                out = np.empty(CHUNK, np.uint8)
+                for r in range(3):
+                    for j in range(len(offs)):
+                        i = (j + t + r) % len(offs)
+                        out.fill(0xEE)
+                        gpu.L.mc_archive_decode_chunk(a.a, offs[i], out.ctypes.data, 0)
+                        if sha(out) != g["decoded_sha"][i]:
+                            errors.append((t, r, g["names"][i]))
+            except Exception as e:   # surfaced below
+                errors.append((t, repr(e)))
+
+        threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+    assert not errors, errors[:5]
+
+
 def test_archive_decode_paths(gpu, golden_chunks, tmp_path):
     """decode_chunk, per-block decode_block, read_region(s) on a GPU-built archive."""
     g = golden_chunks
