@@ -535,7 +535,14 @@ int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens
     if (n < 0 || (n && (!blobs || !lens || !out))) return -1;
     Lane *L = lane();
     if (!L) return -1;
-    constexpr int kBlobGroup = 2;
+    // 2 chunks per group when their blobs are small: the link binds, and a
+    // small first group starts it soonest (a q=6 pair is about 0.9 MB, q=3
+    // about 2.0 MB). 8 when two chunks' blobs pass 4 MiB (a q=1 pair is about
+    // 6.7 MB): the decode binds there and larger launches use the GPU better
+    // (q=1, 64 chunks: 34.2 GB/s end to end against 28.2 with 2-chunk groups;
+    // at q=3, 8-chunk groups gave 40.6 against 44.2)
+    constexpr int kBlobGroupMax = 8, kBlobGroupSmall = 2;
+    constexpr uint64_t kBigPairBytes = 4ull << 20;
     bool ok = true;
     for (int k = 0; k < kBlobSlots; ++k) ok = ok && blob_slot_ready(L->pipe[k]);
     uint32_t bad = 0;
@@ -544,14 +551,16 @@ int mc_b200_decode_chunk_blobs(const uint8_t *const *blobs, const uint64_t *lens
         if (u && S.batch.h_status.p) bad += *S.batch.h_status.as<uint32_t>();
         u = 0;
     };
-    for (int c0 = 0, gi = 0; ok && c0 < n; c0 += kBlobGroup, ++gi) {
+    for (int c0 = 0, gi = 0, g = 0; ok && c0 < n; c0 += g, ++gi) {
         BlobSlot &S = L->pipe[gi % kBlobSlots];
-        const int g = std::min(kBlobGroup, n - c0);
+        uint64_t pair = 0;
+        for (int j = c0; j < std::min(n, c0 + kBlobGroupSmall); ++j) pair += blobs[j] ? lens[j] : 0;
+        g = std::min(pair > kBigPairBytes ? kBlobGroupMax : kBlobGroupSmall, n - c0);
         ok = cuda_ok(cudaEventSynchronize(S.done), "event sync");
         if (!ok) break;
         collect(S, used[gi % kBlobSlots]);
         uint64_t total = 0;
-        uint64_t at[kBlobGroup];
+        uint64_t at[kBlobGroupMax];
         for (int j = 0; j < g; ++j) {
             at[j] = total;
             total += blobs[c0 + j] ? ((lens[c0 + j] + 15) & ~15ull) : 0;
