@@ -340,7 +340,7 @@ def run_serve(args):
             "config": {"workload": f"serving over a {VOLUME_DIMS[2]}x{VOLUME_DIMS[1]}x{VOLUME_DIMS[0]} u8 volume, "
                                    f"LOD 0-3, q={args.q:g}, {nch} chunks",
                        "mix": "70% 16^3 blocks, 20% 128^3 regions, 10% 256^3 chunks",
-                       "locality": "Zipf(1.1) over 128^3 cells", "cache": "8 GiB HBM decoded-block cache, FIFO",
+                       "locality": "Zipf(1.1) over 128^3 cells", "cache": "8 GiB HBM decoded-block cache, S3-FIFO",
                        "classes": "requests up to 256 KiB of output batched on a high-priority stream, larger ones "
                                   "on a normal stream",
                        "outputs": "device memory", "batch_bytes": 512 << 20,

@@ -293,8 +293,9 @@ int mc_b200_append_pyramid(mc_archive *a, const mc_u8 *d_vol, int nz, int ny, in
  * into its output and completes the tickets. Small requests (up to 256 KiB
  * of output: blocks, small regions) and large ones queue and batch apart, on
  * a high-priority and a normal CUDA stream, so a block never waits for a
- * chunk decode in its own batch. Eviction is FIFO over slots no batch in
- * flight is using. Results are byte-identical to
+ * chunk decode in its own batch. Eviction follows the reference's S3-FIFO
+ * (small and main FIFOs, a ghost queue of evicted keys) over slots no batch
+ * in flight is using. Results are byte-identical to
  * mc_archive_decode_block / read_region / decode_chunk.
  *
  * out_on_device: request outputs are DEVICE pointers (any strides for

@@ -5,8 +5,8 @@
 // arena of decoded blocks, a hash from block id to slot and S3-FIFO eviction,
 // with misses decoded on the CPU one block at a time. Here the slot arena is a
 // device buffer, the hash lives on the host beside the archive's node tables,
-// eviction is FIFO over unpinned slots, and misses are decoded on the GPU in
-// batches:
+// eviction follows the same S3-FIFO rules over slots no batch in flight
+// holds, and misses are decoded on the GPU in batches:
 //
 //   submit()  queues a request and returns a ticket;
 //   worker    forms a batch from a queue head while the batch's output bytes
@@ -115,11 +115,17 @@ struct mc_b200_server {
     mc_archive *a = nullptr;
     bool dev_out = true;
     size_t batch_bytes = 0;
-    // decoded-block cache: slots of 4096 bytes, FIFO hand
+    // decoded-block cache: slots of 4096 bytes under S3-FIFO (see take_slot)
     uint8_t *d_cache = nullptr;
-    uint32_t nslots = 0, hand = 0, pinned_slots = 0;
+    uint32_t nslots = 0, pinned_slots = 0;
     std::vector<ChunkRes *> slot_owner;
     std::vector<uint16_t> slot_block;
+    std::vector<uint32_t> free_slots;            // never used yet
+    std::vector<uint8_t> slot_freq;              // reads since the slot's block entered its queue, up to 3
+    std::deque<uint32_t> q_small, q_main;        // every used slot sits in one of the two
+    std::deque<uint64_t> ghost;                  // keys evicted from the small queue, oldest first
+    std::unordered_map<uint64_t, uint32_t> ghost_n;   // how often each key is in `ghost`
+    size_t ghost_cap = 0;
     // per-chunk slot tables (device) and their owners
     uint32_t *d_tables = nullptr;
     uint32_t ntables = 0;
@@ -235,17 +241,64 @@ void release_slot(mc_b200_server *S, uint32_t s) {
     S->st_evict++;
 }
 
-// Next slot in FIFO order whose chunk no batch holds; the caller has checked
-// that one exists.
+// A block's cache key: its chunk's blob offset and its index in the chunk.
+uint64_t block_key(const ChunkRes *c, uint32_t bi) { return c->co * (uint64_t)kGrid3 + bi; }
+
+void ghost_add(mc_b200_server *S, uint64_t key) {
+    if (S->ghost.size() >= S->ghost_cap && !S->ghost.empty()) {
+        auto it = S->ghost_n.find(S->ghost.front());
+        if (it != S->ghost_n.end() && --it->second == 0) S->ghost_n.erase(it);
+        S->ghost.pop_front();
+    }
+    S->ghost.push_back(key);
+    S->ghost_n[key]++;
+}
+
+// A slot for a missing block, under S3-FIFO (the admission and eviction of
+// src/mc_cache.c:300-383, after Yang et al., SOSP 2023): a never-used slot
+// if any; else, while the small queue holds more than a tenth of the slots,
+// its head leaves it -- to the main queue if it was read again or a batch in
+// flight holds its chunk, otherwise evicted, its key remembered in the ghost
+// queue -- and else the main queue's head: kept (its read count lowered) if
+// read or held, otherwise evicted. A held slot is never evicted; the caller
+// has checked that an unheld one exists, and every pass lowers a count, so
+// the loop ends. A slot whose chunk gave up its table is free at once.
 uint32_t take_slot(mc_b200_server *S) {
+    if (!S->free_slots.empty()) {
+        const uint32_t s = S->free_slots.back();
+        S->free_slots.pop_back();
+        return s;
+    }
     for (;;) {
-        const uint32_t s = S->hand;
-        S->hand = S->hand + 1 == S->nslots ? 0 : S->hand + 1;
+        const bool small = S->q_small.size() > S->nslots / 10 || S->q_main.empty();
+        std::deque<uint32_t> &q = small ? S->q_small : S->q_main;
+        const uint32_t s = q.front();
+        q.pop_front();
         ChunkRes *o = S->slot_owner[s];
-        if (o && o->pins) continue;
+        if (!o) return s;
+        if (S->slot_freq[s] > 0 || o->pins) {
+            if (small) S->slot_freq[s] = 0;
+            else if (S->slot_freq[s] > 0) S->slot_freq[s]--;
+            S->q_main.push_back(s);
+            continue;
+        }
+        if (small) ghost_add(S, block_key(o, S->slot_block[s]));
         release_slot(S, s);
         return s;
     }
+}
+
+// A slot just given to block bi of chunk c joins the main queue if the
+// block was evicted from the small queue not long ago, else the small queue.
+void admit_slot(mc_b200_server *S, uint32_t s, const ChunkRes *c, uint32_t bi) {
+    S->slot_freq[s] = 0;
+    if (S->ghost_n.count(block_key(c, bi))) S->q_main.push_back(s);
+    else S->q_small.push_back(s);
+}
+
+// A read of a cached block.
+inline void touch_slot(mc_b200_server *S, uint32_t s) {
+    if (s < kZeroSlot && S->slot_freq[s] < 3) S->slot_freq[s]++;
 }
 
 // The bookkeeping of chunk co, created on first use; when every slot table is
@@ -333,13 +386,22 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
                 std::find(B.waits.begin(), B.waits.end(), std::make_pair(db, db->seq)) == B.waits.end())
                 B.waits.emplace_back(db, db->seq);
             p.g.table = c->table;
-            if (c->resolved == (uint32_t)kGrid3) continue;
+            if (c->resolved == (uint32_t)kGrid3) {   // every block resolved: count the reads
+                for (int bz = p.lo[0] >> 4; bz <= p.hi[0] >> 4; ++bz)
+                    for (int by = p.lo[1] >> 4; by <= p.hi[1] >> 4; ++by)
+                        for (int bx = p.lo[2] >> 4; bx <= p.hi[2] >> 4; ++bx)
+                            touch_slot(S, c->slot[bz << 8 | by << 4 | bx]);
+                continue;
+            }
             const ChunkIndex &ix = chunk_index(a->base, co);
             for (int bz = p.lo[0] >> 4; bz <= p.hi[0] >> 4; ++bz)
                 for (int by = p.lo[1] >> 4; by <= p.hi[1] >> 4; ++by)
                     for (int bx = p.lo[2] >> 4; bx <= p.hi[2] >> 4; ++bx) {
                         const uint32_t bi = (uint32_t)(bz << 8 | by << 4 | bx);
-                        if (c->slot[bi] != kEmptySlot) continue;
+                        if (c->slot[bi] != kEmptySlot) {
+                            touch_slot(S, c->slot[bi]);
+                            continue;
+                        }
                         const uint64_t off = ix.off[bi];
                         if (!off || off + ix.len[bi] > cur) {   // absent block: zeros
                             c->slot[bi] = kZeroSlot;
@@ -366,6 +428,7 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
             const uint32_t bi = m.second;
             if (c->slot[bi] != kEmptySlot) continue;   // the same block twice in one request
             const uint32_t s = take_slot(S);
+            admit_slot(S, s, c, bi);
             c->slot[bi] = s;
             c->resolved++;
             c->resident++;
@@ -603,6 +666,11 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
     if (!cuda_ok(cudaMalloc(&S->d_cache, (size_t)S->nslots * kN3), "cache alloc")) { server_free(S); return nullptr; }
     S->slot_owner.assign(S->nslots, nullptr);
     S->slot_block.assign(S->nslots, 0);
+    S->slot_freq.assign(S->nslots, 0);
+    S->free_slots.reserve(S->nslots);
+    for (uint32_t t = S->nslots; t-- > 0;) S->free_slots.push_back(t);
+    S->ghost_cap = std::max<size_t>(S->nslots - S->nslots / 10, 1);   // as many keys as the main queue's share
+    S->ghost_n.reserve(S->ghost_cap);
     // slot tables: room for every chunk the cache could hold a block of, within reason
     S->ntables = (uint32_t)std::min<size_t>(std::max<size_t>(S->nslots, 1024), 16384);
     if (!cuda_ok(cudaMalloc(&S->d_tables, (size_t)S->ntables * kGrid3 * 4), "table alloc")) {
