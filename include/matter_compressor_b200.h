@@ -300,7 +300,12 @@ int mc_b200_append_pyramid(mc_archive *a, const mc_u8 *d_vol, int nz, int ny, in
  *
  * out_on_device: request outputs are DEVICE pointers (any strides for
  * regions); otherwise HOST pointers (dense outputs only), copied back inside
- * the batch. The archive must not be appended to while the server is open. */
+ * the batch. The archive must not be appended to while the server is open.
+ * cache_bytes is raised to at least one chunk's blocks (16 MiB). A batch in
+ * flight holds every cached block of the chunks it reads; a request whose
+ * chunks' cached blocks leave too few slots for its misses, with no batch in
+ * flight that could free any, is refused (its wait returns -1) rather than
+ * left waiting. */
 typedef struct mc_b200_server mc_b200_server;
 enum { MC_B200_REQ_BLOCK = 0, MC_B200_REQ_REGION = 1, MC_B200_REQ_CHUNK = 2 };
 typedef struct {

@@ -260,25 +260,34 @@ void ghost_add(mc_b200_server *S, uint64_t key) {
 // its head leaves it -- to the main queue if it was read again or a batch in
 // flight holds its chunk, otherwise evicted, its key remembered in the ghost
 // queue -- and else the main queue's head: kept (its read count lowered) if
-// read or held, otherwise evicted. A held slot is never evicted; the caller
-// has checked that an unheld one exists, and every pass lowers a count, so
-// the loop ends. A slot whose chunk gave up its table is free at once.
+// read or held, otherwise evicted. A held slot is never evicted. Once every
+// slot of the main queue has been kept in a row, the small queue is worked
+// whatever its length, so slots held by the batches in flight cannot keep
+// the loop in the main queue. The caller has checked that an unheld slot
+// exists; every pass lowers a read count or shortens the small queue, so the
+// loop ends. A slot whose chunk gave up its table is free at once.
 uint32_t take_slot(mc_b200_server *S) {
     if (!S->free_slots.empty()) {
         const uint32_t s = S->free_slots.back();
         S->free_slots.pop_back();
         return s;
     }
+    size_t main_kept = 0;   // main-queue heads kept in a row
     for (;;) {
-        const bool small = S->q_small.size() > S->nslots / 10 || S->q_main.empty();
+        const bool small = !S->q_small.empty() && (S->q_small.size() > S->nslots / 10 || S->q_main.empty() ||
+                                                   main_kept >= S->q_main.size());
         std::deque<uint32_t> &q = small ? S->q_small : S->q_main;
         const uint32_t s = q.front();
         q.pop_front();
         ChunkRes *o = S->slot_owner[s];
         if (!o) return s;
         if (S->slot_freq[s] > 0 || o->pins) {
-            if (small) S->slot_freq[s] = 0;
-            else if (S->slot_freq[s] > 0) S->slot_freq[s]--;
+            if (small) {
+                S->slot_freq[s] = 0;
+            } else {
+                if (S->slot_freq[s] > 0) S->slot_freq[s]--;
+                ++main_kept;
+            }
             S->q_main.push_back(s);
             continue;
         }
@@ -420,6 +429,20 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
             continue;
         }
         if (no_table || misses.size() > S->nslots - S->pinned_slots) {
+            bool in_flight = false;
+            for (auto &cb : S->batch)
+                for (auto &b : cb) in_flight |= b.busy;
+            if (B.tickets.empty() && !in_flight) {
+                // only this request's own chunks hold the slots it lacks, and
+                // no batch will retire to free any: refuse it rather than wait
+                S->tickets[t].state = -1;
+                qr.pop_front();
+                qt.pop_front();
+                for (ChunkRes *c : B.pins) unpin_chunk(S, c);
+                B.pins.clear();
+                B.waits.clear();
+                continue;
+            }
             if (B.tickets.empty()) S->head_blocked[cls] = true;   // wait until a batch in flight retires
             break;
         }
@@ -662,7 +685,9 @@ mc_b200_server *mc_b200_server_open(mc_archive *a, size_t cache_bytes, size_t ba
     S->a = a;
     S->dev_out = out_on_device != 0;
     S->batch_bytes = batch_bytes ? batch_bytes : ((size_t)256 << 20);
-    S->nslots = (uint32_t)std::min<size_t>(cache_bytes / kN3, 0xFFFFFFF0u);
+    // at least one chunk's blocks: a request whose chunks' cached blocks fill
+    // the cache could otherwise never be admitted
+    S->nslots = (uint32_t)std::min<size_t>(std::max<size_t>(cache_bytes / kN3, kGrid3), 0xFFFFFFF0u);
     if (!cuda_ok(cudaMalloc(&S->d_cache, (size_t)S->nslots * kN3), "cache alloc")) { server_free(S); return nullptr; }
     S->slot_owner.assign(S->nslots, nullptr);
     S->slot_block.assign(S->nslots, 0);

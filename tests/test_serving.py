@@ -217,3 +217,4 @@ def test_small_class_reads_large_class_misses(archive):
             got = run(srv, reqs)
         for r, g in zip(reqs, got):
             assert np.array_equal(g, expected(archive, r)), (trial, r)
+
