@@ -150,8 +150,8 @@ uint32_t mc_b200_last_bad_blocks(void);
  * block on a lane; -1 (the default): by the launch's coded-block count (every
  * block on single threads up to 28 K blocks, the longest 1/64 up to 90 K), and
  * lanes only in the host-blob pipeline, whose groups overlap. Decoded voxels
- * are the same in every case. 0, or -1 for share < -1. No reference
- * counterpart. */
+ * are the same in every case. Returns 0; -1 (with the last error set) for
+ * share < -1 or without a usable device. No reference counterpart. */
 int  mc_b200_set_entropy_solo(int share);
 
 /* Decode n whole chunk blobs held in HOST memory (blob i: blobs[i], blob_lens[i]
