@@ -364,8 +364,8 @@ void mc_b200_server_close(mc_b200_server *s);
  * failure prints one line to stderr.
  *
  * The first call on each device looks up the array's device address and
- * uploads the constant tables, synchronously, with that device current: make
- * it before any stream capture. All calls share the one array, so two calls
+ * uploads the constant tables, synchronously, with that device current. All
+ * calls share the one array, so two calls
  * whose work overlaps on the GPU (other streams, other host threads) race:
  * order them on one stream or with events. */
 int mc_b200_decode_blocks_noalloc(const uint8_t *d_payloads, const uint64_t *h_offsets, int n,
