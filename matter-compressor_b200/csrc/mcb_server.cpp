@@ -438,7 +438,12 @@ void form(mc_b200_server *S, SrvBatch &B, const uint8_t *dbase) {
                 S->tickets[t].state = -1;
                 qr.pop_front();
                 qt.pop_front();
-                for (ChunkRes *c : B.pins) unpin_chunk(S, c);
+                // a later request of this batch that reads one of these chunks
+                // pins it afresh
+                for (ChunkRes *c : B.pins) {
+                    unpin_chunk(S, c);
+                    c->pin_seq = 0;
+                }
                 B.pins.clear();
                 B.waits.clear();
                 continue;

@@ -119,6 +119,35 @@ def test_small_cache_evicts(archive):
     assert st["evictions"] > 0 and st["hits"] > 0
 
 
+def test_region_beyond_a_full_cache_is_refused(archive):
+    """A 16 MiB cache (4096 slots) first filled by one chunk: a region over
+    that chunk and its neighbour needs both chunks' blocks resident at once,
+    more slots than the cache has, so its wait returns -1 rather than waiting
+    for a batch that will never come. The neighbour chunk, submitted right
+    behind it (often into the same batch), and then the first chunk again are
+    served exactly, evicting each other's blocks."""
+    import torch
+    a_req, b_req = (REQ_CHUNK, 0, 0, 0, 0, 0, 0, 0), (REQ_CHUNK, 0, 0, 0, 1, 0, 0, 0)
+    with Server(archive, 16 << 20, 64 << 20) as srv:
+        got_a = run(srv, [a_req])[0]
+        m_a = srv.stats()["misses"]
+        region = torch.empty(256 * 256 * 512, dtype=torch.uint8, device="cuda")
+        out_b = torch.full((CHUNK,), 0xEE, dtype=torch.uint8, device="cuda")
+        t_r = srv.submit(Server.request(REQ_REGION, 0, 0, 0, 0, region.data_ptr(), 256, 256, 512))
+        t_b = srv.submit(Server.request(REQ_CHUNK, 0, 0, 0, 1, out_b.data_ptr()))
+        assert t_r >= 0 and t_b >= 0
+        assert srv.wait(t_r) == -1
+        assert srv.wait(t_b) == 0
+        m_b = srv.stats()["misses"] - m_a
+        again_a = run(srv, [a_req])[0]
+        st = srv.stats()
+    assert m_a < 4096 and m_b < 4096 and m_a + m_b > 4096, (m_a, m_b)
+    assert st["evictions"] > 0
+    want_a = expected(archive, a_req)
+    assert np.array_equal(got_a, want_a) and np.array_equal(again_a, want_a)
+    assert np.array_equal(out_b.cpu().numpy(), expected(archive, b_req))
+
+
 def test_host_outputs(archive):
     rng = np.random.default_rng(8)
     reqs = mixed_requests(rng, 20)
